@@ -1,0 +1,450 @@
+"""ffcm_b200 -- B200 (sm_100a) backend of the FFCM mobility operator.
+
+A host-side mirror of the reference Julia API of ForceCouplingMethod.jl
+(Biofluid-Dynamics-Group/FFCM.jl) over the C ABI of libffcm_b200.so:
+
+=========================================  =========================================
+reference (Julia)                          here (Python)
+=========================================  =========================================
+``FFCMConfig{T}(; L, R_c, N, ...)``        ``FFCMConfig(T, L=..., R_c=..., N=..., ...)``
+``mobility!(V, config, Y, F)``             ``mobility(V, config, Y, F)``
+``FFCMMobility(config, Y)``                ``FFCMMobility(config, Y)``
+``mul!(v, M, f)`` / ``mul!(v, M, f, a, b)``  ``M.mul(v, f)`` / ``M.mul(v, f, a, b)``
+``M * F``                                  ``M @ F`` (also ``M * F``)
+``wrap_positions!`` ... ``correct_velocities!``  same names without ``!``
+=========================================  =========================================
+
+Array convention: a Julia ``3xN`` column-major matrix is a NumPy ``(N, 3)``
+C-order array (the same bytes); shapes are checked in Julia's ``(rows, cols)``
+terms, so an ``(N, 3)`` array is ``3xN``. Arrays may be NumPy arrays (host
+memory; the call copies through the device and returns when V is ready) or
+CUDA ``torch.Tensor`` s of the same shape (device memory; the call is
+asynchronous on the current torch stream). Index buffers are 1-based, as in
+Julia. Errors mirror the reference: ``ArgumentError`` for invalid parameters
+(src/config.jl:288-333), ``DimensionMismatch`` for shapes
+(src/mobility.jl:315-320).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib as L_
+
+__all__ = ["FFCMConfig", "mobility", "FFCMMobility", "ArgumentError", "DimensionMismatch",
+           "FFCMError", "wrap_positions", "assign_cells", "sort_particles_by_cell",
+           "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities"]
+
+
+class ArgumentError(ValueError):
+    """Invalid configuration parameter (Julia ArgumentError)."""
+
+
+class DimensionMismatch(ValueError):
+    """Array shape does not match the configuration (Julia DimensionMismatch)."""
+
+
+class FFCMError(RuntimeError):
+    """CUDA, allocation, timeout or state error reported by the library."""
+
+
+def _raise(code: int):
+    if code == L_.OK:
+        return
+    msg = L_.last_error()
+    if code == L_.ERR_ARGUMENT:
+        raise ArgumentError(msg)
+    if code == L_.ERR_DIMENSION:
+        raise DimensionMismatch(msg)
+    if code == L_.ERR_OOM:
+        raise MemoryError(msg)
+    raise FFCMError(f"[status {code}] {msg}")
+
+
+def _dtype_code(T):
+    T = np.dtype(T)
+    if T == np.float32:
+        return L_.FLOAT32
+    if T == np.float64:
+        return L_.FLOAT64
+    raise ArgumentError(f"working precision must be Float32 or Float64; got {T}")
+
+
+def _dptr(vals):
+    arr = (ctypes.c_double * len(vals))(*[float(v) for v in vals])
+    return arr
+
+
+def _i32ptr(vals):
+    return (ctypes.c_int32 * len(vals))(*[int(v) for v in vals])
+
+
+def _is_torch(x):
+    return type(x).__module__.startswith("torch")
+
+
+def _julia_size(x):
+    """Julia (rows, cols) of an (N, 3)-style row-major array."""
+    shape = tuple(x.shape)
+    if len(shape) == 2:
+        return shape[1], shape[0]
+    if len(shape) == 1:
+        return shape[0], 1
+    return (-1, -1)
+
+
+class _Arg:
+    """A particle array handed to the C ABI (pointer, memory kind, keep-alive)."""
+
+    def __init__(self, x, T, writable=False):
+        self.src = x
+        if _is_torch(x):
+            import torch
+            if x.dtype != (torch.float32 if T == np.float32 else torch.float64):
+                raise ArgumentError(f"tensor dtype {x.dtype} does not match the config's {np.dtype(T)}")
+            if not x.is_contiguous():
+                raise ArgumentError("tensors must be contiguous")
+            self.memory = L_.DEVICE if x.is_cuda else L_.HOST
+            self.ptr = x.data_ptr()
+            self.buf = x
+            self.copy_back = None
+        else:
+            a = np.asarray(x)
+            if a.dtype != np.dtype(T):
+                raise ArgumentError(f"array dtype {a.dtype} does not match the config's {np.dtype(T)}")
+            if writable:
+                if not a.flags.c_contiguous or not a.flags.writeable:
+                    raise ArgumentError("V must be a writable C-contiguous array")
+                buf = a
+            else:
+                buf = np.ascontiguousarray(a)
+            self.memory = L_.HOST
+            self.ptr = buf.ctypes.data
+            self.buf = buf
+        self.rows, self.cols = _julia_size(x)
+
+
+def _stream_of(*args):
+    for a in args:
+        if a is not None and a.memory == L_.DEVICE:
+            import torch
+            return ctypes.c_void_p(torch.cuda.current_stream(a.src.device).cuda_stream)
+    return None
+
+
+class FFCMConfig:
+    """B200 counterpart of ``FFCMConfig{T}`` (src/config.jl:487-558).
+
+    Validates the parameters exactly as the reference (same order, same
+    ArgumentError conditions), derives the scalars in precision ``T`` and
+    allocates every hot-path buffer on ``device``. ``N`` is fixed at
+    construction. ``fft_planning`` and ``fft_threads`` are validated and then
+    have no effect (they configure FFTW on the reference's CPU backend).
+    ``gpu_acceleration`` must be true: this configuration always lives on the
+    GPU; the CPU backend is the reference's own.
+    """
+
+    def __init__(self, T=np.float32, *, L, R_c, N, a=1.0, kernel_widths_ratio,
+                 num_grid_points, M_G, viscosity, fft_planning="measure", fft_threads=1,
+                 gpu_acceleration=True, device=0):
+        self._h = None
+        self.T = np.dtype(T).type
+        dt = _dtype_code(T)
+        if not gpu_acceleration:
+            raise ArgumentError("this backend builds configurations on the GPU only; "
+                                "use the reference CPU backend for gpu_acceleration = false")
+        if fft_planning not in L_.FFT_PLANNING:
+            raise ArgumentError(f"fft_planning must be :estimate, :measure, or :patient; got "
+                                f":{fft_planning}")
+        lib = L_.load()
+        Lp = _dptr(L)
+        Mp = _i32ptr(num_grid_points)
+        h = ctypes.c_void_p()
+        _raise(lib.ffcm_create(ctypes.byref(h), dt, Lp, float(R_c), int(N), float(a),
+                               float(kernel_widths_ratio), Mp, int(M_G), float(viscosity),
+                               L_.FFT_PLANNING[fft_planning], int(fft_threads), int(device)))
+        self._h = h
+        self.device = int(device)
+        self.N = int(N)
+        T_ = self.T
+        self.L = tuple(T_(x) for x in L)
+        self.R_c = T_(R_c)
+        self.a = T_(a)
+        self.mu = T_(viscosity)
+        self.num_grid_points = tuple(int(m) for m in num_grid_points)
+        self.M_G = int(M_G)
+        nc = (ctypes.c_int32 * 3)()
+        cs = (ctypes.c_double * 3)()
+        ics = (ctypes.c_double * 3)()
+        s, S, hh, ih = (ctypes.c_double() for _ in range(4))
+        _raise(lib.ffcm_derive_scalars(dt, Lp, float(R_c), float(a), float(kernel_widths_ratio),
+                                       Mp, nc, cs, ics, ctypes.byref(s), ctypes.byref(S),
+                                       ctypes.byref(hh), ctypes.byref(ih)))
+        self.num_cells = tuple(int(v) for v in nc)
+        self.cell_size = tuple(T_(v) for v in cs)
+        self.inv_cell_size = tuple(T_(v) for v in ics)
+        self.sigma, self.Sigma = T_(s.value), T_(S.value)
+        self.h, self.inv_h = T_(hh.value), T_(ih.value)
+        self.num_cells_total = int(np.prod(self.num_cells))
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            L_.load().ffcm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise FFCMError("configuration has been closed")
+        return self._h
+
+    # -- buffers in the reference layouts --------------------------------
+    def _buf_shape(self, name):
+        N, M, nc = self.N, self.num_grid_points, self.num_cells_total
+        T = self.T
+        return {
+            "Y_WRAPPED": ((N, 3), T), "Y_SORTED": ((N, 3), T), "F_SORTED": ((N, 3), T),
+            "CELL_HASH": ((N,), np.int32), "ORIGINAL_INDEX": ((N,), np.int32),
+            "CELL_START": ((nc,), np.int32), "CELL_END": ((nc,), np.int32),
+            "FORCE_DENSITY": ((3, M[2], M[1], M[0]), T),
+            "FLUID_VELOCITY": ((3, M[2], M[1], M[0]), T),
+            "K_X": ((M[0] // 2 + 1,), T), "K_Y": ((M[1],), T), "K_Z": ((M[2],), T),
+            "NEIGHBOR_MAP": ((13 * nc,), np.int32),
+        }[name]
+
+    def get(self, name):
+        """Copy a configuration buffer to a new NumPy array (reference layout)."""
+        name = name.upper()
+        shape, dt = self._buf_shape(name)
+        out = np.empty(shape, dt)
+        _raise(L_.load().ffcm_get_buffer(self.handle, L_.BUF[name], out.ctypes.data, out.nbytes,
+                                         L_.HOST, None))
+        return out
+
+    def set(self, name, value):
+        """Overwrite a configuration buffer from a NumPy array (reference layout)."""
+        name = name.upper()
+        shape, dt = self._buf_shape(name)
+        arr = np.ascontiguousarray(np.asarray(value, dt).reshape(shape))
+        _raise(L_.load().ffcm_set_buffer(self.handle, L_.BUF[name], arr.ctypes.data, arr.nbytes,
+                                         L_.HOST, None))
+
+    # reference-style accessors
+    cell_hash = property(lambda self: self.get("CELL_HASH"))
+    original_index = property(lambda self: self.get("ORIGINAL_INDEX"))
+    cell_start = property(lambda self: self.get("CELL_START"))
+    cell_end = property(lambda self: self.get("CELL_END"))
+    Y_wrapped = property(lambda self: self.get("Y_WRAPPED"))
+    Y_sorted = property(lambda self: self.get("Y_SORTED"))
+    F_sorted = property(lambda self: self.get("F_SORTED"))
+    force_density = property(lambda self: self.get("FORCE_DENSITY"))
+    fluid_velocity = property(lambda self: self.get("FLUID_VELOCITY"))
+    k_x = property(lambda self: self.get("K_X"))
+    k_y = property(lambda self: self.get("K_Y"))
+    k_z = property(lambda self: self.get("K_Z"))
+
+    # -- measurement --------------------------------------------------------
+    def profile_begin(self):
+        _raise(L_.load().ffcm_profile_begin(self.handle))
+
+    def profile_end(self):
+        ms = (ctypes.c_double * len(L_.STAGES))()
+        calls = (ctypes.c_int64 * len(L_.STAGES))()
+        _raise(L_.load().ffcm_profile_end(self.handle, ms, calls))
+        return {name: (ms[i], calls[i]) for i, name in enumerate(L_.STAGES)}
+
+    def launch_count(self):
+        return int(L_.load().ffcm_launch_count(self.handle))
+
+    def synchronize(self):
+        _raise(L_.load().ffcm_synchronize(self.handle, None))
+
+
+def mobility(V, config: FFCMConfig, Y, F, stream=None):
+    """``mobility!(V, config, Y, F) -> V`` (src/mobility.jl:309-331).
+
+    Overwrites V with the velocities induced by forces F at positions Y, in
+    the caller's original particle order. Y and F are never modified.
+    ``stream`` (a cudaStream_t as int, or a torch.cuda.Stream) overrides the
+    stream the call runs on: by default the current torch stream for CUDA
+    tensors and the configuration's own stream for host arrays.
+    """
+    T = config.T
+    for x in (V, Y, F):
+        if len(getattr(x, "shape", ())) != 2:
+            raise DimensionMismatch(
+                f"V, Y, and F must each be 3xN for the config's N = {config.N}")
+    v = _Arg(V, T, writable=True)
+    y = _Arg(Y, T)
+    f = _Arg(F, T)
+    if len({v.memory, y.memory, f.memory}) != 1:
+        raise ArgumentError("V, Y and F must all be host arrays or all be CUDA tensors")
+    if stream is None:
+        st = _stream_of(v)
+    else:
+        st = ctypes.c_void_p(getattr(stream, "cuda_stream", stream))
+    _raise(L_.load().ffcm_mobility(config.handle, v.ptr, v.rows, v.cols, y.ptr, y.rows, y.cols,
+                                   f.ptr, f.rows, f.cols, v.memory, st))
+    return V
+
+
+# ---- the six steps (reference src/cell_list.jl ... src/correct_velocities.jl) ----
+
+def wrap_positions(config: FFCMConfig, Y):
+    """``wrap_positions!(config.particles.Y_wrapped, Y, config.L)``."""
+    y = _Arg(Y, config.T)
+    if (y.rows, y.cols) != (3, config.N):
+        raise DimensionMismatch("Y must be 3xN")
+    _raise(L_.load().ffcm_wrap_positions(config.handle, y.ptr, y.memory, _stream_of(y)))
+    return config
+
+
+def assign_cells(config: FFCMConfig):
+    """``assign_cells!(config, config.particles.Y_wrapped)``."""
+    _raise(L_.load().ffcm_assign_cells(config.handle, None))
+    return config
+
+
+def sort_particles_by_cell(config: FFCMConfig, F):
+    """``sort_particles_by_cell!(config, config.particles.Y_wrapped, F)``."""
+    f = _Arg(F, config.T)
+    if (f.rows, f.cols) != (3, config.N):
+        raise DimensionMismatch("F must be 3xN")
+    _raise(L_.load().ffcm_sort_particles_by_cell(config.handle, f.ptr, f.memory, _stream_of(f)))
+    return config
+
+
+def spread_forces(config: FFCMConfig):
+    """``spread_forces!(config)``."""
+    _raise(L_.load().ffcm_spread_forces(config.handle, None))
+    return config
+
+
+def stokes_solve(config: FFCMConfig):
+    """``stokes_solve!(config)``."""
+    _raise(L_.load().ffcm_stokes_solve(config.handle, None))
+    return config
+
+
+def interpolate_velocities(V, config: FFCMConfig):
+    """``interpolate_velocities!(V, config)`` (overwrites V, original order)."""
+    v = _Arg(V, config.T, writable=True)
+    if (v.rows, v.cols) != (3, config.N):
+        raise DimensionMismatch("V must be 3xN")
+    _raise(L_.load().ffcm_interpolate_velocities(config.handle, v.ptr, v.memory, _stream_of(v)))
+    return V
+
+
+def correct_velocities(V, config: FFCMConfig):
+    """``correct_velocities!(V, config)`` (adds to V)."""
+    v = _Arg(V, config.T, writable=True)
+    if (v.rows, v.cols) != (3, config.N):
+        raise DimensionMismatch("V must be 3xN")
+    _raise(L_.load().ffcm_correct_velocities(config.handle, v.ptr, v.memory, _stream_of(v)))
+    return V
+
+
+class FFCMMobility:
+    """Matrix-free operator ``FFCMMobility(config, Y)`` (src/mobility.jl:374-448).
+
+    ``size`` is ``(3N, 3N)`` on the flat column-major view (entry 3(n-1)+i is
+    axis i of particle n). ``mul(v, f)`` applies it, ``mul(v, f, alpha, beta)``
+    computes ``alpha*M*f + beta*v`` (beta = 0 overwrites v, ignoring NaN
+    contents), ``M @ F`` maps a 3xN force array to a fresh velocity array.
+    Symmetric positive-definite by construction.
+    """
+
+    def __init__(self, config: FFCMConfig, Y):
+        Y = np.asarray(Y)
+        r, c = _julia_size(Y)
+        if r != 3:
+            raise ArgumentError(f"Y must be 3xN; got size ({r}, {c})")
+        if c != config.N:
+            raise ArgumentError(f"Y has {c} particles but config was built for {config.N}; "
+                                "construct a config with matching N")
+        self.config = config
+        self.Y = np.ascontiguousarray(Y, config.T).copy()
+        self.F_scratch = np.empty((config.N, 3), config.T)
+        self.V_scratch = np.empty((config.N, 3), config.T)
+
+    @property
+    def shape(self):
+        n = 3 * self.config.N
+        return (n, n)
+
+    def size(self, d=None):
+        n = 3 * self.config.N
+        if d is None:
+            return (n, n)
+        return n if d <= 2 else 1
+
+    @property
+    def dtype(self):
+        return np.dtype(self.config.T)
+
+    def mul(self, v, f, alpha=None, beta=None):
+        T = self.config.T
+        self.F_scratch[...] = np.asarray(f, T).reshape(self.config.N, 3)
+        mobility(self.V_scratch, self.config, self.Y, self.F_scratch)
+        out = self.V_scratch.reshape(-1)
+        if alpha is None and beta is None:
+            v[...] = out
+            return v
+        a = T(1 if alpha is None else alpha)
+        b = T(0 if beta is None else beta)
+        if b == 0:
+            v[...] = a * out
+        else:
+            v[...] = a * out + b * v
+        return v
+
+    def __matmul__(self, F):
+        V = np.empty((self.config.N, 3), self.config.T)
+        return mobility(V, self.config, self.Y, F)
+
+    __mul__ = __matmul__
+
+    @staticmethod
+    def issymmetric():
+        return True
+
+    @staticmethod
+    def isposdef():
+        return True
+
+
+def validate_config(T, *, L, R_c, N, a=1.0, kernel_widths_ratio, num_grid_points, M_G,
+                    viscosity, fft_planning="measure", fft_threads=1):
+    """Host-only validation (no device work): raises as FFCMConfig would."""
+    if fft_planning not in L_.FFT_PLANNING:
+        raise ArgumentError(f"fft_planning must be :estimate, :measure, or :patient; got "
+                            f":{fft_planning}")
+    _raise(L_.load().ffcm_validate_config(
+        _dtype_code(T), _dptr(L), float(R_c), int(N), float(a), float(kernel_widths_ratio),
+        _i32ptr(num_grid_points), int(M_G), float(viscosity), L_.FFT_PLANNING[fft_planning],
+        int(fft_threads)))
+
+
+def derive_scalars(T, *, L, R_c, a=1.0, kernel_widths_ratio, num_grid_points):
+    """Host-only derived scalars (``_derive_scalars``), returned in precision T."""
+    T_ = np.dtype(T).type
+    nc = (ctypes.c_int32 * 3)()
+    cs = (ctypes.c_double * 3)()
+    ics = (ctypes.c_double * 3)()
+    s, S, hh, ih = (ctypes.c_double() for _ in range(4))
+    _raise(L_.load().ffcm_derive_scalars(
+        _dtype_code(T), _dptr(L), float(R_c), float(a), float(kernel_widths_ratio),
+        _i32ptr(num_grid_points), nc, cs, ics, ctypes.byref(s), ctypes.byref(S),
+        ctypes.byref(hh), ctypes.byref(ih)))
+    return dict(num_cells=tuple(int(v) for v in nc), cell_size=tuple(T_(v) for v in cs),
+                inv_cell_size=tuple(T_(v) for v in ics), sigma=T_(s.value), Sigma=T_(S.value),
+                h=T_(hh.value), inv_h=T_(ih.value))

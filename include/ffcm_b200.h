@@ -1,0 +1,198 @@
+/*
+ * libffcm_b200 -- C ABI of the B200 (sm_100a) FFCM mobility library.
+ *
+ * The library is the device backend of the reference Julia package
+ * ForceCouplingMethod.jl (Biofluid-Dynamics-Group/FFCM.jl). Every entry point
+ * below replaces one reference function on the hot path; the citation after
+ * each declaration names it (file:line inside the reference project). Julia
+ * binds these with `ccall`; any other host binds them with its C FFI.
+ *
+ * Conventions
+ *  - Every call returns an int status (FFCM_OK = 0). On failure the message is
+ *    available from ffcm_last_error() (thread-local, valid until the next call
+ *    on the same thread).
+ *  - Scalars are passed as double; for FFCM_FLOAT32 handles the library rounds
+ *    them to float exactly once, as Julia's `T(x)` does, so a Float32 caller
+ *    passing its Float32 values gets bit-identical derived scalars.
+ *  - Particle arrays are the reference's 3xN column-major matrices: N
+ *    consecutive (x, y, z) triples of the handle's element type.
+ *  - `memory` says whether a pointer is host (FFCM_HOST) or device
+ *    (FFCM_DEVICE) memory. Host calls copy through the handle and return after
+ *    the result is in host memory; device calls are asynchronous on `stream`.
+ *  - `stream` is a cudaStream_t (NULL = the handle's own stream).
+ *  - Index buffers exchanged through ffcm_get_buffer/ffcm_set_buffer are
+ *    1-based, as in the reference (`original_index`, `cell_start`,
+ *    `cell_end`); cell hashes are 0-based as in the reference.
+ *  - A handle is not re-entrant: one host thread at a time, as the reference
+ *    FFCMConfig (src/config.jl:155-160).
+ */
+#ifndef FFCM_B200_H
+#define FFCM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define FFCM_OK 0
+#define FFCM_ERR_ARGUMENT 1    /* Julia ArgumentError (src/config.jl:288-333)      */
+#define FFCM_ERR_DIMENSION 2   /* Julia DimensionMismatch (src/mobility.jl:315-320) */
+#define FFCM_ERR_OOM 3         /* device or host allocation failed                 */
+#define FFCM_ERR_CUDA 4        /* CUDA runtime error                                */
+#define FFCM_ERR_TIMEOUT 5     /* a bounded device-side wait gave up                */
+#define FFCM_ERR_UNSUPPORTED 6 /* valid for the reference, not for this backend     */
+#define FFCM_ERR_STATE 7       /* null handle, or a step called out of order        */
+
+/* ---- element types ------------------------------------------------------ */
+#define FFCM_FLOAT32 0
+#define FFCM_FLOAT64 1
+
+/* ---- fft_planning (src/config.jl:189-193); accepted and validated only ---- */
+#define FFCM_FFT_ESTIMATE 0
+#define FFCM_FFT_MEASURE 1
+#define FFCM_FFT_PATIENT 2
+
+/* ---- memory kinds -------------------------------------------------------- */
+#define FFCM_HOST 0
+#define FFCM_DEVICE 1
+
+/* ---- buffers reachable by ffcm_get_buffer / ffcm_set_buffer --------------
+ * Sizes in elements; T is the handle's element type.                        */
+#define FFCM_BUF_Y_WRAPPED 0      /* 3N T    particles.Y_wrapped (src/config.jl:75-82)   */
+#define FFCM_BUF_Y_SORTED 1       /* 3N T    particles.Y_sorted                          */
+#define FFCM_BUF_F_SORTED 2       /* 3N T    particles.F_sorted                          */
+#define FFCM_BUF_CELL_HASH 3      /* N int32 cells.cell_hash, 0-based (src/config.jl:45-52) */
+#define FFCM_BUF_ORIGINAL_INDEX 4 /* N int32 cells.original_index, 1-based               */
+#define FFCM_BUF_CELL_START 5     /* ncell int32, 1-based inclusive                      */
+#define FFCM_BUF_CELL_END 6       /* ncell int32, 1-based inclusive (empty: end=start-1) */
+#define FFCM_BUF_FORCE_DENSITY 7  /* 3*Mx*My*Mz T, grid.force_density, x fastest, SoA    */
+#define FFCM_BUF_FLUID_VELOCITY 8 /* 3*Mx*My*Mz T, grid.fluid_velocity                   */
+#define FFCM_BUF_K_X 9            /* Mx/2+1 T  solver.k_x (src/config.jl:374-377)        */
+#define FFCM_BUF_K_Y 10           /* My T      solver.k_y                                */
+#define FFCM_BUF_K_Z 11           /* Mz T      solver.k_z                                */
+#define FFCM_BUF_NEIGHBOR_MAP 12  /* 13*ncell int32, half-shell map, 0-based, get only
+                                     (src/cell_list.jl:258-289)                          */
+#define FFCM_BUF_COUNT 13
+
+/* ---- profiling stages (ffcm_profile_end) --------------------------------- */
+#define FFCM_STAGE_H2D 0
+#define FFCM_STAGE_CELL_LIST 1
+#define FFCM_STAGE_SPREAD 2
+#define FFCM_STAGE_FFT_X_FWD 3
+#define FFCM_STAGE_FFT_Y_FWD 4
+#define FFCM_STAGE_FFT_Z_STOKES 5
+#define FFCM_STAGE_FFT_Y_INV 6
+#define FFCM_STAGE_FFT_X_INV 7
+#define FFCM_STAGE_INTERPOLATE 8
+#define FFCM_STAGE_CORRECT 9
+#define FFCM_STAGE_D2H 10
+#define FFCM_STAGE_COUNT 11
+
+typedef struct ffcm_handle ffcm_handle;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* ffcm_last_error(void);
+
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int ffcm_version(void);
+
+/* Parameter validation of the cold path, no device work.
+ * Replaces _validate_config_parameters + the anisotropy check of
+ * _derive_scalars (src/config.jl:288-333, 362-369). */
+int ffcm_validate_config(int32_t dtype, const double* L, double R_c, int64_t N, double a,
+                         double kernel_widths_ratio, const int32_t* num_grid_points,
+                         int32_t M_G, double viscosity, int32_t fft_planning,
+                         int32_t fft_threads);
+
+/* Derived scalars in the working precision (returned widened to double,
+ * exactly). Replaces _derive_scalars (src/config.jl:347-380); lets the Julia
+ * side cache them in its FFCMConfig fields. Any output pointer may be NULL. */
+int ffcm_derive_scalars(int32_t dtype, const double* L, double R_c, double a,
+                        double kernel_widths_ratio, const int32_t* num_grid_points,
+                        int32_t* num_cells /*3*/, double* cell_size /*3*/,
+                        double* inv_cell_size /*3*/, double* sigma, double* Sigma, double* h,
+                        double* inv_h);
+
+/* Build a configuration on `device`: validates, derives scalars, allocates
+ * every hot-path buffer and the FFT tables. Replaces the GPU arm of
+ * FFCMConfig{T}(...) (src/config.jl:487-558; ext/ForceCouplingMethodCUDAExt/
+ * config.jl:19-103). */
+int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, int64_t N,
+                double a, double kernel_widths_ratio, const int32_t* num_grid_points,
+                int32_t M_G, double viscosity, int32_t fft_planning, int32_t fft_threads,
+                int32_t device);
+
+/* Release a configuration (finalizer of FFCMConfig). */
+int ffcm_destroy(ffcm_handle* h);
+
+/* Particle count, element type and cell count of a handle. */
+int ffcm_get_info(const ffcm_handle* h, int64_t* N, int32_t* dtype, int64_t* num_cells_total);
+
+/* The assembled operator V = M^VF(Y) F. Replaces mobility!(V, config, Y, F)
+ * (src/mobility.jl:309-331) including its staging seam
+ * (ext/ForceCouplingMethodCUDAExt/mobility.jl:10-23). Shapes are Julia's
+ * (rows, cols) of V, Y, F; anything but (3, N) is FFCM_ERR_DIMENSION. Y and F
+ * are never written; V is overwritten in the caller's original order. */
+int ffcm_mobility(ffcm_handle* h, void* V, int64_t v_rows, int64_t v_cols, const void* Y,
+                  int64_t y_rows, int64_t y_cols, const void* F, int64_t f_rows,
+                  int64_t f_cols, int32_t memory, void* stream);
+
+/* ---- the six steps, for step-isolated parity ----------------------------- */
+
+/* Y_wrapped = mod.(Y, L). Replaces wrap_positions!(Y_wrapped, Y, L)
+ * (src/cell_list.jl:22-31). */
+int ffcm_wrap_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stream);
+
+/* cell_hash from Y_wrapped. Replaces assign_cells! (src/cell_list.jl:193-238). */
+int ffcm_assign_cells(ffcm_handle* h, void* stream);
+
+/* Stable counting sort by cell_hash, cell ranges, and gather of Y_wrapped and
+ * F into sorted order. Replaces sort_particles_by_cell!(config, Y_wrapped, F)
+ * (src/cell_list.jl:119-176). */
+int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, void* stream);
+
+/* force_density from Y_sorted/F_sorted. Replaces spread_forces!
+ * (src/spread_forces.jl:17-130). */
+int ffcm_spread_forces(ffcm_handle* h, void* stream);
+
+/* fluid_velocity = L^-1 force_density. Replaces stokes_solve!
+ * (src/stokes_solve.jl:151-240). */
+int ffcm_stokes_solve(ffcm_handle* h, void* stream);
+
+/* V[:, original_index[s]] = h^3 * gather. Replaces interpolate_velocities!
+ * (src/interpolate.jl:263-376). V is 3xN. */
+int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream);
+
+/* V += self and pair correction. Replaces correct_velocities!
+ * (src/correct_velocities.jl:154-286). V is 3xN. */
+int ffcm_correct_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream);
+
+/* ---- buffer access (step isolation, as test/cuda/ does) ------------------ */
+int64_t ffcm_buffer_bytes(const ffcm_handle* h, int32_t which);
+int ffcm_get_buffer(ffcm_handle* h, int32_t which, void* dst, int64_t nbytes, int32_t memory,
+                    void* stream);
+int ffcm_set_buffer(ffcm_handle* h, int32_t which, const void* src, int64_t nbytes,
+                    int32_t memory, void* stream);
+
+/* Wait for the handle's work on `stream` and report any sticky device-side
+ * error (non-finite position, a bounded wait that gave up). */
+int ffcm_synchronize(ffcm_handle* h, void* stream);
+
+/* ---- measurement --------------------------------------------------------- */
+
+/* Start recording CUDA events around every stage of every call. */
+int ffcm_profile_begin(ffcm_handle* h);
+/* Stop recording; waits for the recorded work and returns, per stage, the
+ * summed milliseconds and the number of timed launches (arrays of
+ * FFCM_STAGE_COUNT). */
+int ffcm_profile_end(ffcm_handle* h, double* stage_ms, int64_t* stage_calls);
+/* Number of kernels this handle has launched since creation. */
+int64_t ffcm_launch_count(const ffcm_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFCM_B200_H */

@@ -90,9 +90,10 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None):
         cc = np.minimum((cand / cs).astype(np.int64), nc - 1)
         ok = np.ones(B, bool)
         # against kept centres
+        cu = max(1, int(fill.max()))
         for o in offs:
             nb = (cc + o) % nc
-            occ = grid[nb[:, 0], nb[:, 1], nb[:, 2]]          # (B, cap)
+            occ = grid[nb[:, 0], nb[:, 1], nb[:, 2], :cu]     # (B, cu)
             valid = occ >= 0
             if not valid.any():
                 continue
@@ -130,15 +131,19 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None):
                     bad[a[conflict]] = True
             ok &= ~bad
         acc = np.nonzero(ok)[0][:need]
-        for q in acc:
-            c = cc[q]
-            k = fill[c[0], c[1], c[2]]
-            if k >= cap:
-                continue
-            grid[c[0], c[1], c[2], k] = count
-            fill[c[0], c[1], c[2]] = k + 1
-            pos[count] = cand[q]
-            count += 1
+        if acc.size:
+            flat = (cc[acc, 0] * nc + cc[acc, 1]) * nc + cc[acc, 2]
+            order = np.argsort(flat, kind="stable")
+            acc, flat = acc[order], flat[order]
+            first = np.searchsorted(flat, flat)             # first index of each cell group
+            slot = fill.reshape(-1)[flat] + (np.arange(flat.size) - first)
+            keep = slot < cap
+            acc, flat, slot = acc[keep], flat[keep], slot[keep]
+            ids = count + np.arange(acc.size)
+            grid.reshape(-1, cap)[flat, slot] = ids
+            np.maximum.at(fill.reshape(-1), flat, slot + 1)
+            pos[count:count + acc.size] = cand[acc]
+            count += acc.size
     perm = rng.permutation(N)
     return pos[perm]
 

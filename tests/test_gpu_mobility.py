@@ -1,0 +1,240 @@
+"""End-to-end parity of the assembled operator (mobility!, FFCMMobility) on the
+GPU through the C ABI, against the committed golden fixtures, the live oracle,
+and the reference's own known answers (test/cuda/test_gpu_mobility.jl,
+test/accuracy/test_single_sphere_mobility.jl, test_mobility.jl,
+test_mobility_properties.jl). At the full N = 500k / 512^3 size the checks are
+the oracle comparison plus size-independent properties (linearity, symmetry,
+positivity, determinism of the permutation)."""
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import ffcm_oracle as O
+from fixtures import clustered_cloud, nonoverlapping_uniform, random_cloud
+from gpu_helpers import both, kw_of, rel_l2
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+TS = [np.float32, np.float64]
+
+
+def _run(ffcm, cfg, Y, F):
+    V = np.empty((cfg.N, 3), cfg.T)
+    ffcm.mobility(V, cfg, Y, F)
+    return V
+
+
+@pytest.mark.parametrize("name", ["standard_random256", "c1_N2000_64"])
+@pytest.mark.parametrize("tag,T", [("f32", np.float32), ("f64", np.float64)])
+def test_mobility_matches_golden(ffcm, name, tag, T):
+    z = np.load(GOLDEN / f"{name}.npz")
+    Lb, N, M, MG, Rc, ratio = z["meta"]
+    cfg = ffcm.FFCMConfig(T, **kw_of(Lb, int(N), int(M), M_G=int(MG), R_c=Rc, ratio=ratio))
+    V = _run(ffcm, cfg, z[f"{tag}_Y"], z[f"{tag}_F"])
+    assert np.array_equal(cfg.original_index, z[f"{tag}_original_index"])
+    assert np.array_equal(cfg.cell_start, z[f"{tag}_cell_start"])
+    assert np.array_equal(cfg.cell_end, z[f"{tag}_cell_end"])
+    ref = z[f"{tag}_V"]
+    if T == np.float32:
+        assert rel_l2(V, ref) < 1e-5                       # vs the Float32 oracle
+        assert rel_l2(V, z["f64_V"]) < 1e-4                # vs the Float64 oracle
+        np.testing.assert_allclose(V, ref, rtol=np.sqrt(np.finfo(T).eps), atol=1e-6)
+    else:
+        assert rel_l2(V, ref) < 1e-10
+        np.testing.assert_allclose(V, ref, rtol=1e-8, atol=1e-10)
+
+
+@pytest.mark.parametrize("T", TS)
+def test_mobility_reference_gpu_cases(ffcm, T):
+    """test/cuda/test_gpu_mobility.jl:29-55: single sphere, cluster, random cloud."""
+    L = 8.0
+    cases = [
+        (1, (np.array([[4.0, 4.0, 4.0]], T), np.array([[1.0, 0.0, 0.0]], T))),
+        (64, clustered_cloud(T, 64)),
+        (256, random_cloud(T, 256, (L, L, L), 0xC7A0)),
+    ]
+    for N, (Y, F) in cases:
+        prod, ora = both(ffcm, T, **kw_of(L, N, 16))
+        Vg = _run(ffcm, prod, Y, F)
+        Vo = O.apply(ora, Y, F)
+        np.testing.assert_allclose(Vg, Vo, rtol=np.sqrt(np.finfo(T).eps),
+                                   atol=1e-6 if T == np.float32 else 1e-10)
+
+
+def test_single_sphere_lattice_sum_on_gpu(ffcm):
+    """test_single_sphere_mobility.jl: Σ/σ = 1, M_G = 21, 32^3, rtol 1e-5 (steps 1-5),
+    then Σ/σ = 1.25, 1.5 with all six steps, rtol 1e-4, Σ-independent."""
+    T = np.float64
+    cfg = ffcm.FFCMConfig(T, **kw_of(8.0, 1, 32, M_G=21, ratio=1.0))
+    Y = np.array([[4.0, 4.0, 4.0]])
+    F = np.array([[1.0, 0.0, 0.0]])
+    ffcm.wrap_positions(cfg, Y)
+    ffcm.assign_cells(cfg)
+    ffcm.sort_particles_by_cell(cfg, F)
+    ffcm.spread_forces(cfg)
+    ffcm.stokes_solve(cfg)
+    V = np.zeros((1, 3))
+    ffcm.interpolate_velocities(V, cfg)
+    ref = O.periodic_self_mobility_xx(1 / np.sqrt(np.pi), 1.0, 8.0)
+    assert V[0, 0] == pytest.approx(ref, rel=1e-5)
+    assert abs(V[0, 1]) < 1e-12 and abs(V[0, 2]) < 1e-12
+    vs = []
+    for ratio in (1.25, 1.5):
+        c = ffcm.FFCMConfig(T, **kw_of(8.0, 1, 32, M_G=31, ratio=ratio))
+        V = _run(ffcm, c, Y, F)
+        assert V[0, 0] == pytest.approx(ref, rel=1e-4)
+        assert abs(V[0, 1]) < 1e-10 and abs(V[0, 2]) < 1e-10
+        vs.append(V[0, 0])
+    assert vs[0] == pytest.approx(vs[1], rel=1e-4)
+
+
+@pytest.mark.parametrize("T", TS)
+def test_operator_contracts(ffcm, T):
+    """test_mobility.jl: inputs untouched, DimensionMismatch, linearity, SPD,
+    FFCMMobility mul!/5-arg/M*F, traits."""
+    cfg = ffcm.FFCMConfig(T, **kw_of(8.0, 4, 16))
+    Y = np.array([[9.3, 4.0, 4.0], [4.1, 4.2, 4.0], [-0.4, 4.0, 4.0], [4.0, 9.9, 4.0]], T)
+    F = np.array([[0.5, -0.1, 0.2], [-0.3, 0.4, 0.1], [0.2, 0.0, 0.7], [0.1, 0.3, -0.5]], T)
+    Y0, F0 = Y.copy(), F.copy()
+    V = _run(ffcm, cfg, Y, F)
+    assert (Y == Y0).all() and (F == F0).all()
+    for bad in (np.zeros((5, 3), T), np.zeros((4, 2), T)):
+        with pytest.raises(ffcm.DimensionMismatch):
+            ffcm.mobility(bad.copy(), cfg, Y, F)
+        with pytest.raises(ffcm.DimensionMismatch):
+            ffcm.mobility(np.zeros((4, 3), T), cfg, bad, F)
+        with pytest.raises(ffcm.DimensionMismatch):
+            ffcm.mobility(np.zeros((4, 3), T), cfg, Y, bad)
+    G = np.array([[0.1, 0.3, -0.2], [0.2, -0.5, 0.4], [-0.4, 0.6, 0.1], [0.3, 0.2, 0.1]], T)
+    a, b = T(1.7), T(-0.9)
+    r, at = np.sqrt(np.finfo(T).eps), (1e-6 if T == np.float32 else 1e-10)
+    np.testing.assert_allclose(_run(ffcm, cfg, Y, a * F + b * G),
+                               a * V + b * _run(ffcm, cfg, Y, G), rtol=r, atol=at)
+    M = ffcm.FFCMMobility(cfg, Y)
+    assert M.size() == (12, 12) and M.shape == (12, 12) and M.dtype == np.dtype(T)
+    assert M.issymmetric() and M.isposdef()
+    v = np.zeros(12, T)
+    M.mul(v, F.reshape(-1))
+    np.testing.assert_allclose(v, V.reshape(-1), rtol=r, atol=at)
+    v0 = (np.arange(1, 13) * 0.1).astype(T)
+    v = v0.copy()
+    M.mul(v, F.reshape(-1), T(2), T(-0.5))
+    np.testing.assert_allclose(v, 2 * V.reshape(-1) - 0.5 * v0, rtol=r, atol=at)
+    vn = np.full(12, np.nan, T)
+    M.mul(vn, F.reshape(-1), T(2), T(0))
+    assert np.isfinite(vn).all()
+    np.testing.assert_allclose(M @ F, V, rtol=r, atol=at)
+    with pytest.raises(ffcm.DimensionMismatch):
+        M @ np.zeros((5, 3), T)
+    Fg = np.array([[0.5, -0.1, 0.2], [-0.3, 0.4, 0.6], [0.1, 0.1, 0.1], [0.0, 0.2, -0.3]], T)
+    VF, VG = _run(ffcm, cfg, Y, Fg), _run(ffcm, cfg, Y, G)
+    assert np.sum(G * VF, dtype=np.float64) == pytest.approx(np.sum(Fg * VG, dtype=np.float64), rel=r)
+    assert np.sum(Fg * VF, dtype=np.float64) > 0
+
+
+@pytest.mark.parametrize("T", TS)
+def test_mobility_identities_random_configurations(ffcm, T):
+    """test_mobility_properties.jl (NumPy seed 2024), compared with the oracle too."""
+    rng = np.random.default_rng(2024)
+    r, at = np.sqrt(np.finfo(T).eps), (1e-6 if T == np.float32 else 1e-10)
+    for _ in range(6):
+        M = tuple(int(rng.choice([8, 10, 12, 14, 16])) for _ in range(3))
+        L = tuple(0.5 * m for m in M)
+        N = int(rng.integers(2, 9))
+        kw = dict(L=L, R_c=1.0, N=N, kernel_widths_ratio=float(1 + 1.5 * rng.random()),
+                  viscosity=float(0.5 + 2 * rng.random()), num_grid_points=M,
+                  M_G=int(rng.integers(6, min(M) + 1)))
+        prod, ora = both(ffcm, T, **kw)
+        Y = np.array([[(3 * rng.random() - 1) * L[i] for i in range(3)] for _ in range(N)], T)
+        F = (2 * rng.random((N, 3)) - 1).astype(T)
+        G = (2 * rng.random((N, 3)) - 1).astype(T)
+        a, b = T(2 * rng.random() - 1), T(2 * rng.random() - 1)
+        VF, VG = _run(ffcm, prod, Y, F), _run(ffcm, prod, Y, G)
+        np.testing.assert_allclose(_run(ffcm, prod, Y, a * F + b * G), a * VF + b * VG,
+                                   rtol=r, atol=at)
+        assert np.sum(G * VF, dtype=np.float64) == pytest.approx(
+            np.sum(F * VG, dtype=np.float64), rel=r, abs=at)
+        assert np.sum(F * VF, dtype=np.float64) > 0
+        np.testing.assert_allclose(VF, O.apply(ora, Y, F), rtol=r, atol=at)
+
+
+def test_nonfinite_position_is_an_argument_error(ffcm):
+    cfg = ffcm.FFCMConfig(np.float32, **kw_of(8.0, 3, 16))
+    Y = np.array([[1, 1, 1], [np.nan, 2, 2], [3, 3, 3]], np.float32)
+    F = np.ones((3, 3), np.float32)
+    with pytest.raises(ffcm.ArgumentError):
+        ffcm.mobility(np.zeros((3, 3), np.float32), cfg, Y, F)
+    Y[1, 0] = 2.0          # the configuration stays usable
+    V = _run(ffcm, cfg, Y, F)
+    assert np.isfinite(V).all()
+
+
+@pytest.mark.parametrize("T", TS)
+def test_device_pointer_path_matches_host_path(ffcm, T):
+    torch = pytest.importorskip("torch")
+    z = np.load(GOLDEN / "c1_N2000_64.npz")
+    tag = "f32" if T == np.float32 else "f64"
+    cfg = ffcm.FFCMConfig(T, **kw_of(40.0, 2000, 64, R_c=3.0))
+    Vh = _run(ffcm, cfg, z[f"{tag}_Y"], z[f"{tag}_F"])
+    Yd = torch.from_numpy(z[f"{tag}_Y"]).cuda()
+    Fd = torch.from_numpy(z[f"{tag}_F"]).cuda()
+    Vd = torch.empty_like(Yd)
+    ffcm.mobility(Vd, cfg, Yd, Fd)
+    torch.cuda.synchronize()
+    cfg.synchronize()
+    assert np.array_equal(Vd.cpu().numpy(), Vh) or rel_l2(Vd.cpu().numpy(), Vh) < 1e-6
+
+
+# ---- the headline configuration: N = 500k, 512^3 --------------------------
+@pytest.fixture(scope="module")
+def c2_inputs():
+    L, N = 275.6, 500_000
+    Y = nonoverlapping_uniform(N, L, 2024 + 1)
+    F = np.random.default_rng(2024 + 1).standard_normal((N, 3))
+    return L, N, Y, F
+
+
+def test_c2_full_size_against_oracle(ffcm, c2_inputs):
+    """N = 500k, L = 275.6, 512^3 Float32 against the Float32 and Float64 oracles
+    (the oracle finishes this in tens of seconds on the host)."""
+    L, N, Y, F = c2_inputs
+    kw = kw_of(L, N, 512, R_c=3.0)
+    prod = ffcm.FFCMConfig(np.float32, **kw)
+    Y32, F32 = Y.astype(np.float32), F.astype(np.float32)
+    Vg = _run(ffcm, prod, Y32, F32)
+    o32 = O.OracleConfig(np.float32, **kw)
+    o32.fft_threads = 8
+    V32 = O.apply(o32, Y32, F32)
+    assert np.array_equal(prod.original_index, o32.original_index)
+    assert rel_l2(Vg, V32) < 1e-5
+    o64 = O.OracleConfig(np.float64, **kw)
+    o64.fft_threads = 8
+    V64 = O.apply(o64, Y32.astype(np.float64), F32.astype(np.float64))
+    assert rel_l2(Vg, V64) < 1e-4
+
+
+def test_c2_full_size_properties(ffcm, c2_inputs):
+    L, N, Y, F = c2_inputs
+    cfg = ffcm.FFCMConfig(np.float32, **kw_of(L, N, 512, R_c=3.0))
+    Y32 = Y.astype(np.float32)
+    F32 = F.astype(np.float32)
+    G32 = np.random.default_rng(77).standard_normal((N, 3)).astype(np.float32)
+    VF = _run(ffcm, cfg, Y32, F32)
+    perm1 = cfg.original_index
+    VF2 = _run(ffcm, cfg, Y32, F32)
+    assert np.array_equal(cfg.original_index, perm1)         # deterministic sort
+    assert rel_l2(VF2, VF) < 1e-6                             # atomic-order floor
+    h = cfg.cell_hash[perm1 - 1]
+    assert (np.diff(h) >= 0).all()                            # grouped by cell
+    same = np.diff(h) == 0
+    assert (np.diff(perm1)[same] > 0).all()                   # stable inside cells
+    VG = _run(ffcm, cfg, Y32, G32)
+    a, b = np.float32(0.7), np.float32(-1.3)
+    Vc = _run(ffcm, cfg, Y32, a * F32 + b * G32)
+    assert rel_l2(Vc, a * VF + b * VG) < 1e-5                 # linearity
+    s1 = np.sum(G32.astype(np.float64) * VF)
+    s2 = np.sum(F32.astype(np.float64) * VG)
+    assert abs(s1 - s2) <= 1e-4 * np.sqrt(np.sum(F32.astype(np.float64) * VF) *
+                                          np.sum(G32.astype(np.float64) * VG))  # symmetry
+    assert np.sum(F32.astype(np.float64) * VF) > 0            # positivity
