@@ -27,7 +27,6 @@ Julia. Errors mirror the reference: ``ArgumentError`` for invalid parameters
 from __future__ import annotations
 
 import ctypes
-import math
 
 import numpy as np
 
@@ -126,11 +125,22 @@ class _Arg:
         self.rows, self.cols = _julia_size(x)
 
 
+# cudaStreamLegacy: the legacy default stream. torch reports its default stream
+# as handle 0, which the C ABI reads as "the configuration's own stream".
+_CUDA_STREAM_LEGACY = 1
+
+
+def _stream_handle(s):
+    """A cudaStream_t for the C ABI from a torch stream or a raw handle."""
+    h = int(getattr(s, "cuda_stream", s) or 0)
+    return ctypes.c_void_p(h if h != 0 else _CUDA_STREAM_LEGACY)
+
+
 def _stream_of(*args):
     for a in args:
         if a is not None and a.memory == L_.DEVICE:
             import torch
-            return ctypes.c_void_p(torch.cuda.current_stream(a.src.device).cuda_stream)
+            return _stream_handle(torch.cuda.current_stream(a.src.device))
     return None
 
 
@@ -291,7 +301,7 @@ def mobility(V, config: FFCMConfig, Y, F, stream=None):
     if stream is None:
         st = _stream_of(v)
     else:
-        st = ctypes.c_void_p(getattr(stream, "cuda_stream", stream))
+        st = _stream_handle(stream)
     _raise(L_.load().ffcm_mobility(config.handle, v.ptr, v.rows, v.cols, y.ptr, y.rows, y.cols,
                                    f.ptr, f.rows, f.cols, v.memory, st))
     return V

@@ -185,4 +185,14 @@ __global__ void k_cell_order_gather(int ncell, const int32_t* __restrict__ off,
     }
 }
 
+// Re-gather forces only (a further right-hand side on the same positions).
+template <typename T>
+__global__ void k_gather_forces(int n_part, const int32_t* __restrict__ perm, const T* __restrict__ F,
+                                vec4<T>* __restrict__ Fs) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_part; s += gridDim.x * blockDim.x) {
+        const int64_t n = perm[s];
+        Fs[s] = vec4<T>{F[3 * n], F[3 * n + 1], F[3 * n + 2], T(0)};
+    }
+}
+
 }  // namespace ffcm

@@ -18,33 +18,35 @@
 namespace ffcm {
 
 // Constants of _correction_scalars that do not depend on r, computed on the
-// host in the working precision with the reference's operation order.
+// host in the working precision. The pair scalars below are the reference's
+// expressions regrouped over powers of 1/r (one division per pair instead of
+// fifteen); they agree with the reference to round-off.
 template <typename T>
 struct CorrConsts {
-    T s2, s4, S2, S4, d, dq, fourpimu, eightpimu, mu;
-    T two_sigma, two_Sigma, pref_s, pref_S, four_s2, four_S2;
+    T inv_two_sigma, inv_two_Sigma, pref_s, pref_S, inv_four_s2, inv_four_S2;
+    T k1, k2, k3, k4, k5, k6, k7, k8, k9, k10, k11, k12, k13;
     T self;
     T L0, L1, L2, Rc2, ic0, ic1, ic2;
     int m0, m1, m2;
 };
 
+// src/correct_velocities.jl:71-104:
+//   A = erf_diff (1/(8 pi mu r) + s2/(4 pi mu r^3)) - 2 s4/(mu r^2) D_s
+//       + [2 S4/(mu r^2) + d/mu (1 + 2 S2/r^2) - dq (2 - r^2/(2 S2))/(2 mu S2)] D_S
+//   B = erf_diff (1/(8 pi mu r^3) - 3 s2/(4 pi mu r^5)) + 6 s4/(mu r^4) D_s
+//       + [-6 S4/(mu r^4) - d/(mu r^2) (1 + 6 S2/r^2) - dq/(4 mu S4)] D_S
 template <typename T>
 __device__ __forceinline__ void correction_scalars(T r, const CorrConsts<T>& c, T& A, T& B) {
     const T r2 = r * r;
-    const T r3 = r * r * r;
-    const T r4 = r2 * r2;
-    const T r5 = r4 * r;
-    const T erf_diff = erf_t(r / c.two_sigma) - erf_t(r / c.two_Sigma);
-    const T Ds = c.pref_s * exp_t(-r2 / c.four_s2);
-    const T DS = c.pref_S * exp_t(-r2 / c.four_S2);
-    A = erf_diff * (T(1) / (c.eightpimu * r) + c.s2 / (c.fourpimu * r3)) -
-        T(2) * c.s4 / (c.mu * r2) * Ds +
-        (T(2) * c.S4 / (c.mu * r2) + c.d / c.mu * (T(1) + T(2) * c.S2 / r2) -
-         c.dq * (T(2) - r2 / (T(2) * c.S2)) / (T(2) * c.mu * c.S2)) * DS;
-    B = erf_diff * (T(1) / (c.eightpimu * r3) - T(3) * c.s2 / (c.fourpimu * r5)) +
-        T(6) * c.s4 / (c.mu * r4) * Ds +
-        (-T(6) * c.S4 / (c.mu * r4) - c.d / (c.mu * r2) * (T(1) + T(6) * c.S2 / r2) -
-         c.dq / (T(4) * c.mu * c.S4)) * DS;
+    const T ir = T(1) / r;
+    const T ir2 = ir * ir, ir3 = ir2 * ir, ir4 = ir2 * ir2, ir5 = ir4 * ir;
+    const T erf_diff = erf_t(r * c.inv_two_sigma) - erf_t(r * c.inv_two_Sigma);
+    const T Ds = c.pref_s * exp_t(-r2 * c.inv_four_s2);
+    const T DS = c.pref_S * exp_t(-r2 * c.inv_four_S2);
+    A = erf_diff * (c.k1 * ir + c.k2 * ir3) - c.k3 * ir2 * Ds +
+        (c.k4 * ir2 + c.k5 * (T(1) + c.k6 * ir2) - c.k7 * (T(2) - r2 * c.k8)) * DS;
+    B = erf_diff * (c.k1 * ir3 - c.k9 * ir5) + c.k10 * ir4 * Ds +
+        (-c.k11 * ir4 - c.k5 * ir2 * (T(1) + c.k12 * ir2) - c.k13) * DS;
 }
 
 template <typename T>
@@ -52,10 +54,14 @@ __device__ __forceinline__ T min_image(T x, T L) {
     return sub_rn(x, mul_rn(L, rint_t(div_rn(x, L))));
 }
 
+// Vs == nullptr: V[:, perm[s]] += dv (the step API, reference semantics).
+// Vs != nullptr: V[:, perm[s]] = h3 * Vs[s] + dv (finishes the fused
+// interpolation, which left its sums in sorted order in Vs).
 template <typename T>
 __global__ void k_correct(int n_part, const vec4<T>* __restrict__ Ys,
                           const vec4<T>* __restrict__ Fs, const int32_t* __restrict__ off,
-                          const int32_t* __restrict__ perm, T* __restrict__ V, CorrConsts<T> c) {
+                          const int32_t* __restrict__ perm, T* __restrict__ V, CorrConsts<T> c,
+                          const T* __restrict__ Vs, T h3) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_part; s += gridDim.x * blockDim.x) {
         const vec4<T> yn = Ys[s];
         const vec4<T> fn = Fs[s];
@@ -95,9 +101,15 @@ __global__ void k_correct(int n_part, const vec4<T>* __restrict__ Ys,
             }
         }
         const int64_t n = perm[s];
-        V[3 * n] += v0;
-        V[3 * n + 1] += v1;
-        V[3 * n + 2] += v2;
+        if (Vs) {
+            V[3 * n] = h3 * Vs[3 * (int64_t)s] + v0;
+            V[3 * n + 1] = h3 * Vs[3 * (int64_t)s + 1] + v1;
+            V[3 * n + 2] = h3 * Vs[3 * (int64_t)s + 2] + v2;
+        } else {
+            V[3 * n] += v0;
+            V[3 * n + 1] += v1;
+            V[3 * n + 2] += v2;
+        }
     }
 }
 

@@ -6,6 +6,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <cstdlib>
+#include <functional>
 #include <memory>
 #include <string>
 #include <vector>
@@ -15,6 +17,9 @@
 #include "cell_list.cuh"
 #include "correct.cuh"
 #include "fft.cuh"
+#include "fft_dispatch.cuh"
+#include "fft_pipe.cuh"
+#include "slab.cuh"
 #include "spread_interp.cuh"
 
 using namespace ffcm;
@@ -184,6 +189,10 @@ struct EngineBase {
     virtual int stokes(cudaStream_t s) = 0;
     virtual int interp(void* V, cudaStream_t s) = 0;
     virtual int correct(void* V, cudaStream_t s) = 0;
+    virtual int mobility_rest(void* V, cudaStream_t s) = 0;
+    virtual int gather_forces(const void* F, cudaStream_t s) = 0;
+    virtual int ensure_real_grids() = 0;
+    virtual bool uses_slab() const = 0;
     virtual void* Y_in() = 0;
     virtual void* F_in() = 0;
     virtual void* V_out() = 0;
@@ -271,6 +280,21 @@ struct Engine final : EngineBase {
     FftPlan plan_x, plan_y, plan_z;
     int lpb_x, tx_y, tx_z;
     size_t smem_x, smem_y, smem_z, smem_stencil;
+    // register (power-of-two) FFT path, per axis
+    bool fast_x = false, fast_y = false, fast_z = false;
+    int lpb_fx = 0, By = 0, Bz = 0;
+    // y/z pass variant: 0 = one tile per block (k_fftp_*), 1 = persistent
+    // pipelined (k_fftq_*); grid size of the persistent variant
+    int ykind = 0, zkind = 0, ygrid = 0, zgrid = 0;
+    int num_sms = 148;
+    size_t smem_fx = 0, smem_fy = 0, smem_fz = 0;
+    // slab kernels: spread/interpolation fused with the x transforms
+    bool slab = false;
+    SlabKernels<T> sk;
+    SlabGeom sg;
+    T* partial = nullptr;
+    int* slab_lists = nullptr;   // per-slab particle lists kept by the spread
+    int* slab_counts = nullptr;
     int ntiles;
 
     T *Yin = nullptr, *Fin = nullptr, *Vout = nullptr, *Yw = nullptr;
@@ -329,24 +353,34 @@ struct Engine final : EngineBase {
         // correction constants (src/correct_velocities.jl:21-27, 71-104)
         const T pi = T(kPi);
         const T s2 = d.sigma * d.sigma;
-        cc.s2 = s2; cc.s4 = s2 * s2; cc.S2 = S2; cc.S4 = S4;
-        cc.d = s2 - S2;
-        cc.dq = cc.d * cc.d / T(4);
-        cc.fourpimu = T(4) * pi * mu;
-        cc.eightpimu = T(8) * pi * mu;
-        cc.mu = mu;
-        cc.two_sigma = T(2) * d.sigma;
-        cc.two_Sigma = T(2) * d.Sigma;
+        const T s4 = s2 * s2;
+        const T dd2 = s2 - S2;
+        const T dq = dd2 * dd2 / T(4);
+        cc.inv_two_sigma = T(1) / (T(2) * d.sigma);
+        cc.inv_two_Sigma = T(1) / (T(2) * d.Sigma);
         cc.pref_s = std::pow(T(4) * pi * s2, -T(3) / T(2));
         cc.pref_S = std::pow(T(4) * pi * S2, -T(3) / T(2));
-        cc.four_s2 = T(4) * s2;
-        cc.four_S2 = T(4) * S2;
+        cc.inv_four_s2 = T(1) / (T(4) * s2);
+        cc.inv_four_S2 = T(1) / (T(4) * S2);
+        cc.k1 = T(1) / (T(8) * pi * mu);
+        cc.k2 = s2 / (T(4) * pi * mu);
+        cc.k3 = T(2) * s4 / mu;
+        cc.k4 = T(2) * S4 / mu;
+        cc.k5 = dd2 / mu;
+        cc.k6 = T(2) * S2;
+        cc.k7 = dq / (T(2) * mu * S2);
+        cc.k8 = T(1) / (T(2) * S2);
+        cc.k9 = T(3) * s2 / (T(4) * pi * mu);
+        cc.k10 = T(6) * s4 / mu;
+        cc.k11 = T(6) * S4 / mu;
+        cc.k12 = T(6) * S2;
+        cc.k13 = dq / (T(4) * mu * S4);
         {
             const T a = T(1);
             const T Ssp = d.Sigma * std::sqrt(pi);
             cc.self = T(1) / (T(6) * pi * mu * a) - T(1) / (T(6) * pi * mu * Ssp) +
-                      cc.d / (T(12) * mu * (Ssp * Ssp * Ssp)) -
-                      (cc.d * cc.d) / (T(32) * mu * std::pow(d.Sigma, T(5)) * std::sqrt(pi * pi * pi));
+                      dd2 / (T(12) * mu * (Ssp * Ssp * Ssp)) -
+                      (dd2 * dd2) / (T(32) * mu * std::pow(d.Sigma, T(5)) * std::sqrt(pi * pi * pi));
         }
         cc.L0 = L[0]; cc.L1 = L[1]; cc.L2 = L[2];
         const T R = T(R_c);
@@ -370,6 +404,67 @@ struct Engine final : EngineBase {
         if (smem_x > budget || smem_y > budget || smem_z > budget)
             return fail(FFCM_ERR_UNSUPPORTED, "grid dimension too large for the shared-memory FFT");
         smem_stencil = 8 * 3 * (size_t)MG * (2 * sizeof(T) + sizeof(int));
+        fast_x = xeven && fast_len(Mx / 2);
+        fast_y = fast_len(My);
+        fast_z = fast_len(Mz);
+        if (fast_x) {
+            lpb_fx = FastFft<T>::x_lpb(Mx / 2);
+            smem_fx = FastFft<T>::x_smem(Mx / 2);
+            CUDA_TRY(cudaFuncSetAttribute(xf_kernel<T>(Mx / 2), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fx));
+            CUDA_TRY(cudaFuncSetAttribute(xi_kernel<T>(Mx / 2), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fx));
+        }
+        auto max_cell_rows = [&](int B, double cs) {
+            const double span = (double)(B + MG - 1 + 1) * (double)d.h + 2e-3 * (double)d.h;
+            return (int)std::ceil(span / cs) + 1;
+        };
+        if (fast_x && slab_kernels<T>(Mx / 2, sk) && My % sk.BY == 0 && Mz % sk.BZ == 0 &&
+            MG == SLAB_MG &&
+            (int64_t)std::min(max_cell_rows(sk.BY, (double)d.cell_size[1]), m1) *
+                    std::min(max_cell_rows(sk.BZ, (double)d.cell_size[2]), m2) <= SLAB_PAIRMAX &&
+            std::getenv("FFCM_NO_SLAB") == nullptr) {
+            slab = true;
+            sg.m0 = m0; sg.m1 = m1; sg.m2 = m2;
+            sg.cs1 = (double)d.cell_size[1];
+            sg.cs2 = (double)d.cell_size[2];
+            sg.h = (double)d.h;
+            sg.nty = My / sk.BY;
+            sg.ntz = Mz / sk.BZ;
+            // expected touching particles per slab: N x (rows reached)/(rows total)
+            const double expect = (double)N * (sk.BY + MG - 1) * (sk.BZ + MG - 1) / ((double)My * Mz);
+            sg.lcap = (int)std::min<double>(1 << 20, std::max(256.0, 4.0 * expect + 64.0));
+            sg.lcap = (sg.lcap + 31) / 32 * 32;
+            CUDA_TRY(cudaFuncSetAttribute(sk.spread_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sk.smem));
+            CUDA_TRY(cudaFuncSetAttribute(sk.interp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sk.smem));
+        }
+        if (fast_y) {
+            int cand[4];
+            const int nc = y_bundles(My, cand);
+            for (int i = 0; i < nc; ++i)
+                CUDA_TRY(cudaFuncSetAttribute(y_kernel<T>(My, cand[i]), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)FastFft<T>::yz_smem(My, cand[i])));
+            By = cand[nc - 1];
+        }
+        if (fast_z) {
+            int cand[4];
+            const int nc = z_bundles(Mz, cand);
+            for (int i = 0; i < nc; ++i)
+                CUDA_TRY(cudaFuncSetAttribute(z_kernel<T>(Mz, cand[i]), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)FastFft<T>::yz_smem(Mz, cand[i])));
+            Bz = cand[nc - 1];
+        }
+        {
+            int dev = 0;
+            CUDA_TRY(cudaGetDevice(&dev));
+            CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+        }
+        for (int B : {2, 4, 8, 16}) {
+            if (fast_y && ypipe_kernel<T>(My, B) && hxp % B == 0 && ypipe_smem<T>(My, B) <= budget)
+                CUDA_TRY(cudaFuncSetAttribute(ypipe_kernel<T>(My, B), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)ypipe_smem<T>(My, B)));
+            if (fast_z && zpipe_kernel<T>(Mz, B) && hxp % B == 0 && zpipe_smem<T>(Mz, B) <= budget)
+                CUDA_TRY(cudaFuncSetAttribute(zpipe_kernel<T>(Mz, B), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)zpipe_smem<T>(Mz, B)));
+        }
         CUDA_TRY(cudaFuncSetAttribute(k_fft_x_r2c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
         CUDA_TRY(cudaFuncSetAttribute(k_fft_x_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
         CUDA_TRY(cudaFuncSetAttribute(k_fft_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
@@ -393,8 +488,6 @@ struct Engine final : EngineBase {
         TRY(alloc(scratch_i, std::max<size_t>(N, (size_t)ncell + 1)));
         TRY(alloc(Ys, N));
         TRY(alloc(Fs, N));
-        TRY(alloc(gf, 3 * (size_t)plane));
-        TRY(alloc(gu, 3 * (size_t)plane));
         TRY(alloc(spec, 3 * (size_t)hxp * My * Mz));
         TRY(alloc(twx, Mx));
         TRY(alloc(twy, My));
@@ -402,10 +495,13 @@ struct Engine final : EngineBase {
         TRY(alloc(kxv, nkx));
         TRY(alloc(kyv, My));
         TRY(alloc(kzv, Mz));
+        if (slab) {
+            TRY(alloc(partial, 3 * (size_t)N));
+            TRY(alloc(slab_lists, (size_t)sg.nty * sg.ntz * sg.lcap));
+            TRY(alloc(slab_counts, (size_t)sg.nty * sg.ntz));
+        }
 
         // zero-initialised grids and cell list (src/config.jl:464-469)
-        CUDA_TRY(cudaMemset(gf, 0, 3 * (size_t)plane * sizeof(T)));
-        CUDA_TRY(cudaMemset(gu, 0, 3 * (size_t)plane * sizeof(T)));
         CUDA_TRY(cudaMemset(spec, 0, 3 * (size_t)hxp * My * Mz * sizeof(cplx<T>)));
         CUDA_TRY(cudaMemset(off, 0, ((size_t)ncell + 1) * sizeof(int32_t)));
         CUDA_TRY(cudaMemset(perm, 0, (size_t)N * sizeof(int32_t)));
@@ -447,7 +543,120 @@ struct Engine final : EngineBase {
         h->kx.assign(kx.begin(), kx.end());
         h->ky.assign(ky.begin(), ky.end());
         h->kz.assign(kz.begin(), kz.end());
+        const char* at = std::getenv("FFCM_AUTOTUNE");
+        if (!(at && at[0] == '0')) TRY(autotune());
         return FFCM_OK;
+    }
+
+    // Launch-shape autotuner: times every instantiated bundle width of the y
+    // and z passes on this configuration's own buffers and keeps the fastest.
+    int time_launches(const std::function<int()>& f, float& ms) {
+        cudaEvent_t a, b;
+        CUDA_TRY(cudaEventCreate(&a));
+        CUDA_TRY(cudaEventCreate(&b));
+        TRY(f());
+        CUDA_TRY(cudaEventRecord(a, h->stream));
+        for (int i = 0; i < 3; ++i) TRY(f());
+        CUDA_TRY(cudaEventRecord(b, h->stream));
+        CUDA_TRY(cudaEventSynchronize(b));
+        CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return FFCM_OK;
+    }
+
+    int persistent_grid(const void* kernel, int threads, size_t smem, int ntiles, int& grid) {
+        int per_sm = 0;
+        CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+        if (per_sm < 1) return fail(FFCM_ERR_UNSUPPORTED, "pipelined FFT kernel does not fit on an SM");
+        grid = std::max(1, std::min(ntiles, per_sm * num_sms));
+        return FFCM_OK;
+    }
+
+    int autotune() {
+        const bool verbose = std::getenv("FFCM_VERBOSE") != nullptr;
+        if (fast_y) {
+            float best = 1e30f;
+            int bk = 0, bB = By, bg = 0;
+            for (int kind = 0; kind < 2; ++kind)
+                for (int B : {2, 4, 8, 16}) {
+                    if (kind == 0 && !y_kernel<T>(My, B)) continue;
+                    if (kind == 1 && !(ypipe_kernel<T>(My, B) && hxp % B == 0 &&
+                                       ypipe_smem<T>(My, B) <= 200 * 1024)) continue;
+                    if (kind == 0) {
+                        int cand[4];
+                        const int nc = y_bundles(My, cand);
+                        bool ok = false;
+                        for (int i = 0; i < nc; ++i) ok |= cand[i] == B;
+                        if (!ok) continue;
+                    }
+                    ykind = kind;
+                    By = B;
+                    if (kind == 1) {
+                        const int ntiles = ((nkx + B - 1) / B) * Mz * 3;
+                        TRY(persistent_grid((const void*)ypipe_kernel<T>(My, B), B * (My / 8),
+                                            ypipe_smem<T>(My, B), ntiles, ygrid));
+                    }
+                    float ms = 0;
+                    TRY(time_launches([&] { return launch_y(h->stream, 0); }, ms));
+                    if (verbose) fprintf(stderr, "ffcm autotune: y n=%d kind=%d B=%d %.4f ms\n", My, kind, B, ms / 3);
+                    if (ms < best) { best = ms; bk = kind; bB = B; bg = ygrid; }
+                }
+            ykind = bk; By = bB; ygrid = bg;
+        }
+        if (fast_z) {
+            float best = 1e30f;
+            int bk = 0, bB = Bz, bg = 0;
+            for (int kind = 0; kind < 2; ++kind)
+                for (int B : {2, 4, 8, 16}) {
+                    if (kind == 0 && !z_kernel<T>(Mz, B)) continue;
+                    if (kind == 1 && !(zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
+                                       zpipe_smem<T>(Mz, B) <= 200 * 1024)) continue;
+                    if (kind == 0) {
+                        int cand[4];
+                        const int nc = z_bundles(Mz, cand);
+                        bool ok = false;
+                        for (int i = 0; i < nc; ++i) ok |= cand[i] == B;
+                        if (!ok) continue;
+                    }
+                    zkind = kind;
+                    Bz = B;
+                    if (kind == 1) {
+                        const int ntiles = ((nkx + B - 1) / B) * My;
+                        TRY(persistent_grid((const void*)zpipe_kernel<T>(Mz, B), B * (Mz / 8),
+                                            zpipe_smem<T>(Mz, B), ntiles, zgrid));
+                    }
+                    float ms = 0;
+                    TRY(time_launches([&] { return launch_z(h->stream); }, ms));
+                    if (verbose) fprintf(stderr, "ffcm autotune: z n=%d kind=%d B=%d %.4f ms\n", Mz, kind, B, ms / 3);
+                    if (ms < best) { best = ms; bk = kind; bB = B; bg = zgrid; }
+                }
+            zkind = bk; Bz = bB; zgrid = bg;
+        }
+        CUDA_TRY(cudaStreamSynchronize(h->stream));
+        h->launches = 0;
+        return FFCM_OK;
+    }
+    int tuned_By = 0, tuned_Bz = 0;
+
+    // The real force-density and velocity grids are needed only by the step
+    // API and by the generic (non-slab) pipeline; they are allocated, zeroed,
+    // on first use.
+    int ensure_real_grids() override {
+        if (gf) return FFCM_OK;
+        TRY(alloc(gf, 3 * (size_t)plane));
+        TRY(alloc(gu, 3 * (size_t)plane));
+        CUDA_TRY(cudaMemset(gf, 0, 3 * (size_t)plane * sizeof(T)));
+        CUDA_TRY(cudaMemset(gu, 0, 3 * (size_t)plane * sizeof(T)));
+        return FFCM_OK;
+    }
+
+    bool uses_slab() const override { return slab; }
+
+    int gather_forces(const void* F, cudaStream_t s) override {
+        StageScope sc(h, FFCM_STAGE_CELL_LIST, s);
+        return launch(h, k_gather_forces<T>, grid_for(N, 256), 256, 0, s, N, (const int32_t*)perm,
+                      static_cast<const T*>(F), Fs);
     }
 
     void* Y_in() override { return Yin; }
@@ -477,44 +686,137 @@ struct Engine final : EngineBase {
                       (const int32_t*)off, perm, (const T*)Yw, static_cast<const T*>(F), Ys, Fs);
     }
 
+    // Hot path of the assembled operator: spread straight into the x-transformed
+    // spectrum, y/z passes, then x-c2r fused with the interpolation.
+    bool fused_available() const { return slab; }
+
+    int spread_to_spectrum(cudaStream_t s) {
+        StageScope sc(h, FFCM_STAGE_SPREAD, s);
+        dim3 g(sg.nty, sg.ntz, 1);
+        return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys, (const vec4<T>*)Fs,
+                      (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, slab_lists,
+                      slab_counts);
+    }
+
+    int stokes_yz(cudaStream_t s) {
+        {
+            StageScope sc(h, FFCM_STAGE_FFT_Y_FWD, s);
+            TRY(launch_y(s, 0));
+        }
+        {
+            StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
+            TRY(launch_z(s));
+        }
+        StageScope sc(h, FFCM_STAGE_FFT_Y_INV, s);
+        return launch_y(s, 1);
+    }
+
+    // x-c2r + gather; leaves h^-3 V in sorted order in `partial` for correct_final.
+    int interp_from_spectrum(cudaStream_t s) {
+        StageScope sc(h, FFCM_STAGE_INTERPOLATE, s);
+        CUDA_TRY(cudaMemsetAsync(partial, 0, 3 * (size_t)N * sizeof(T), s));
+        dim3 g(sg.nty, sg.ntz, 1);
+        return launch(h, sk.interp, g, 256, sk.smem, s, (const vec4<T>*)Ys, (const int32_t*)off,
+                      (const cplx<T>*)spec, hxp, partial, sp, sg, (const cplx<T>*)twx,
+                      (const int*)slab_lists, (const int*)slab_counts);
+    }
+
+    int mobility_rest(void* V, cudaStream_t s) override {
+        if (!slab) {
+            TRY(spread(s));
+            TRY(stokes(s));
+            TRY(interp(V, s));
+            return correct(V, s);
+        }
+        TRY(spread_to_spectrum(s));
+        TRY(stokes_yz(s));
+        TRY(interp_from_spectrum(s));
+        StageScope sc(h, FFCM_STAGE_CORRECT, s);
+        return launch(h, k_correct<T>, grid_for(N, 128), 128, 0, s, N, (const vec4<T>*)Ys,
+                      (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
+                      static_cast<T*>(V), cc, (const T*)partial, h3);
+    }
+
     int spread(cudaStream_t s) override {
+        // step API (spread_forces!): depends on Y_sorted/F_sorted only, as the
+        // reference's, so it does not use the cell-list-driven slab kernel
+        TRY(ensure_real_grids());
         StageScope sc(h, FFCM_STAGE_SPREAD, s);
         CUDA_TRY(cudaMemsetAsync(gf, 0, 3 * (size_t)plane * sizeof(T), s));
         return launch(h, k_spread_atomic<T>, grid_for((int64_t)N * 32, 256, 148 * 64), 256,
                       smem_stencil, s, N, (const vec4<T>*)Ys, (const vec4<T>*)Fs, gf, sp);
     }
 
+    int launch_y(cudaStream_t s, int inverse) {
+        if (fast_y && ykind == 1) {
+            return launch(h, ypipe_kernel<T>(My, By), ygrid, By * (My / 8), ypipe_smem<T>(My, By), s, spec,
+                          nkx, Mz, hxp, (const cplx<T>*)twy, inverse);
+        }
+        if (fast_y) {
+            dim3 g((nkx + By - 1) / By, Mz, 3);
+            return launch(h, y_kernel<T>(My, By), g, By * (My / 8), FastFft<T>::yz_smem(My, By), s, spec,
+                          nkx, My, Mz, hxp, (const cplx<T>*)twy, inverse);
+        }
+        dim3 gy((nkx + tx_y - 1) / tx_y, Mz, 3);
+        return launch(h, k_fft_y<T>, gy, 256, smem_y, s, spec, nkx, My, Mz, hxp, plan_y,
+                      (const cplx<T>*)twy, tx_y, inverse);
+    }
+
+    int launch_z(cudaStream_t s) {
+        if (fast_z && zkind == 1) {
+            return launch(h, zpipe_kernel<T>(Mz, Bz), zgrid, Bz * (Mz / 8), zpipe_smem<T>(Mz, Bz), s, spec,
+                          nkx, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+                          (const T*)kzv, inv_mu_M);
+        }
+        if (fast_z) {
+            dim3 g((nkx + Bz - 1) / Bz, My, 1);
+            return launch(h, z_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::yz_smem(Mz, Bz), s, spec,
+                          nkx, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+                          (const T*)kzv, inv_mu_M);
+        }
+        dim3 gz((nkx + tx_z - 1) / tx_z, My, 1);
+        return launch(h, k_fft_z_stokes<T>, gz, 256, smem_z, s, spec, nkx, My, Mz, hxp, plan_z,
+                      (const cplx<T>*)twz, tx_z, (const T*)kxv, (const T*)kyv, (const T*)kzv, inv_mu_M);
+    }
+
     int stokes(cudaStream_t s) override {
+        TRY(ensure_real_grids());
         const int nrows = 3 * My * Mz;
         {
             StageScope sc(h, FFCM_STAGE_FFT_X_FWD, s);
-            TRY(launch(h, k_fft_x_r2c<T>, (nrows + lpb_x - 1) / lpb_x, 256, smem_x, s,
-                       (const T*)gf, spec, Mx, nrows, hxp, plan_x, (const cplx<T>*)twx, lpb_x));
+            if (fast_x) {
+                const int H = Mx / 2;
+                TRY(launch(h, xf_kernel<T>(H), (nrows + lpb_fx - 1) / lpb_fx, lpb_fx * (H / 8), smem_fx, s,
+                           (const T*)gf, spec, nrows, hxp, (const cplx<T>*)twx, lpb_fx));
+            } else {
+                TRY(launch(h, k_fft_x_r2c<T>, (nrows + lpb_x - 1) / lpb_x, 256, smem_x, s,
+                           (const T*)gf, spec, Mx, nrows, hxp, plan_x, (const cplx<T>*)twx, lpb_x));
+            }
         }
-        dim3 gy((nkx + tx_y - 1) / tx_y, Mz, 3);
         {
             StageScope sc(h, FFCM_STAGE_FFT_Y_FWD, s);
-            TRY(launch(h, k_fft_y<T>, gy, 256, smem_y, s, spec, nkx, My, Mz, hxp, plan_y,
-                       (const cplx<T>*)twy, tx_y, 0));
+            TRY(launch_y(s, 0));
         }
         {
             StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
-            dim3 gz((nkx + tx_z - 1) / tx_z, My, 1);
-            TRY(launch(h, k_fft_z_stokes<T>, gz, 256, smem_z, s, spec, nkx, My, Mz, hxp, plan_z,
-                       (const cplx<T>*)twz, tx_z, (const T*)kxv, (const T*)kyv, (const T*)kzv,
-                       inv_mu_M));
+            TRY(launch_z(s));
         }
         {
             StageScope sc(h, FFCM_STAGE_FFT_Y_INV, s);
-            TRY(launch(h, k_fft_y<T>, gy, 256, smem_y, s, spec, nkx, My, Mz, hxp, plan_y,
-                       (const cplx<T>*)twy, tx_y, 1));
+            TRY(launch_y(s, 1));
         }
         StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
+        if (fast_x) {
+            const int H = Mx / 2;
+            return launch(h, xi_kernel<T>(H), (nrows + lpb_fx - 1) / lpb_fx, lpb_fx * (H / 8), smem_fx, s,
+                          (const cplx<T>*)spec, gu, nrows, hxp, (const cplx<T>*)twx, lpb_fx);
+        }
         return launch(h, k_fft_x_c2r<T>, (nrows + lpb_x - 1) / lpb_x, 256, smem_x, s,
                       (const cplx<T>*)spec, gu, Mx, nrows, hxp, plan_x, (const cplx<T>*)twx, lpb_x);
     }
 
     int interp(void* V, cudaStream_t s) override {
+        TRY(ensure_real_grids());
         StageScope sc(h, FFCM_STAGE_INTERPOLATE, s);
         return launch(h, k_interpolate_warp<T>, grid_for((int64_t)N * 32, 256, 148 * 64), 256,
                       smem_stencil, s, N, (const vec4<T>*)Ys, (const int32_t*)perm,
@@ -525,7 +827,7 @@ struct Engine final : EngineBase {
         StageScope sc(h, FFCM_STAGE_CORRECT, s);
         return launch(h, k_correct<T>, grid_for(N, 128), 128, 0, s, N, (const vec4<T>*)Ys,
                       (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
-                      static_cast<T*>(V), cc);
+                      static_cast<T*>(V), cc, (const T*)nullptr, T(0));
     }
 };
 
@@ -728,10 +1030,7 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
     }
     TRY(e->wrap_hash(Yd, true, true, s));
     TRY(e->sort(Fd, s));
-    TRY(e->spread(s));
-    TRY(e->stokes(s));
-    TRY(e->interp(Vd, s));
-    TRY(e->correct(Vd, s));
+    TRY(e->mobility_rest(Vd, s));
     if (memory == FFCM_HOST) {
         {
             StageScope sc(h, FFCM_STAGE_D2H, s);
@@ -870,8 +1169,8 @@ int buffer_io(ffcm_handle* h, Engine<T>* e, int32_t which, void* ext, int64_t nb
     switch (which) {
         case FFCM_BUF_Y_WRAPPED: TRY(copy(e->Yw)); break;
         case FFCM_BUF_CELL_HASH: TRY(copy(e->key)); break;
-        case FFCM_BUF_FORCE_DENSITY: TRY(copy(e->gf)); break;
-        case FFCM_BUF_FLUID_VELOCITY: TRY(copy(e->gu)); break;
+        case FFCM_BUF_FORCE_DENSITY: TRY(e->ensure_real_grids()); TRY(copy(e->gf)); break;
+        case FFCM_BUF_FLUID_VELOCITY: TRY(e->ensure_real_grids()); TRY(copy(e->gu)); break;
         case FFCM_BUF_Y_SORTED:
         case FFCM_BUF_F_SORTED: {
             vec4<T>* dev = which == FFCM_BUF_Y_SORTED ? e->Ys : e->Fs;
@@ -1007,5 +1306,199 @@ int ffcm_profile_end(ffcm_handle* h, double* stage_ms, int64_t* stage_calls) {
 }
 
 int64_t ffcm_launch_count(const ffcm_handle* h) { return h ? h->launches : -1; }
+
+}  // extern "C"
+
+// ===========================================================================
+// Batched form: many systems x many right-hand sides, one graph launch
+// ===========================================================================
+struct ffcm_batch {
+    int32_t dtype = FFCM_FLOAT32, device = 0, nrhs = 1;
+    int64_t nsys = 0, totalN = 0;
+    size_t esize = 4;
+    std::vector<ffcm_handle*> sys;
+    std::vector<int64_t> N, yoff, fvoff;
+    void* Yb = nullptr;
+    void* Fb = nullptr;
+    void* Vb = nullptr;
+    cudaStream_t main = nullptr;
+    std::vector<cudaStream_t> ws;
+    std::vector<cudaEvent_t> ev;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int64_t kernels = 0;
+};
+
+namespace {
+
+void batch_release(ffcm_batch* b) {
+    if (!b) return;
+    DeviceGuard g(b->device);
+    if (b->main) cudaStreamSynchronize(b->main);
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
+    for (cudaStream_t s : b->ws) cudaStreamDestroy(s);
+    if (b->main) cudaStreamDestroy(b->main);
+    if (b->Yb) cudaFree(b->Yb);
+    if (b->Fb) cudaFree(b->Fb);
+    if (b->Vb) cudaFree(b->Vb);
+    for (ffcm_handle* h : b->sys) ffcm_destroy(h);
+    delete b;
+}
+
+// Capture every system's pipeline (cell list once, then nrhs grid solves) as
+// one dependency branch per system, forked from and joined into b->main.
+int batch_build_graph(ffcm_batch* b) {
+    const size_t es = b->esize;
+    CUDA_TRY(cudaStreamBeginCapture(b->main, cudaStreamCaptureModeThreadLocal));
+    int rc = FFCM_OK;
+    cudaEvent_t fork = b->ev[0];
+    rc = cudaEventRecord(fork, b->main) == cudaSuccess ? FFCM_OK : FFCM_ERR_CUDA;
+    int64_t launches0 = 0;
+    for (ffcm_handle* h : b->sys) launches0 += h->launches;
+    for (int64_t i = 0; i < b->nsys && rc == FFCM_OK; ++i) {
+        cudaStream_t s = b->ws[i];
+        if (cudaStreamWaitEvent(s, fork, 0) != cudaSuccess) { rc = FFCM_ERR_CUDA; break; }
+        EngineBase* e = b->sys[i]->eng.get();
+        const char* Y = static_cast<const char*>(b->Yb) + 3 * b->yoff[i] * es;
+        auto Fr = [&](int r) { return static_cast<const char*>(b->Fb) + (b->fvoff[i] + 3 * r * b->N[i]) * es; };
+        auto Vr = [&](int r) { return static_cast<char*>(b->Vb) + (b->fvoff[i] + 3 * r * b->N[i]) * es; };
+        rc = e->wrap_hash(Y, true, true, s);
+        if (rc == FFCM_OK) rc = e->sort(Fr(0), s);
+        if (rc == FFCM_OK) rc = e->mobility_rest(Vr(0), s);
+        for (int r = 1; r < b->nrhs && rc == FFCM_OK; ++r) {
+            rc = e->gather_forces(Fr(r), s);
+            if (rc == FFCM_OK) rc = e->mobility_rest(Vr(r), s);
+        }
+        if (rc == FFCM_OK && (cudaEventRecord(b->ev[1 + i], s) != cudaSuccess ||
+                              cudaStreamWaitEvent(b->main, b->ev[1 + i], 0) != cudaSuccess))
+            rc = FFCM_ERR_CUDA;
+    }
+    std::string msg = g_err;
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(b->main, &graph);
+    if (rc != FFCM_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return fail(rc, "graph capture failed: " + msg);
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    b->graph = graph;
+    CUDA_TRY(cudaGraphInstantiate(&b->exec, b->graph, 0));
+    int64_t launches1 = 0;
+    for (ffcm_handle* h : b->sys) launches1 += h->launches;
+    b->kernels = launches1 - launches0;
+    return FFCM_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ffcm_batch_create(ffcm_batch** out, int32_t dtype, int64_t nsys, const double* L,
+                      const double* R_c, const int64_t* N, double a, double ratio,
+                      const int32_t* M, int32_t M_G, double mu, int32_t nrhs, int32_t device) {
+    g_err.clear();
+    if (!out) return fail(FFCM_ERR_ARGUMENT, "out must not be NULL");
+    *out = nullptr;
+    if (nsys < 1) return fail(FFCM_ERR_ARGUMENT, "a batch needs at least one system");
+    if (nrhs < 1) return fail(FFCM_ERR_ARGUMENT, "nrhs must be at least 1");
+    if (!L || !R_c || !N || !M) return fail(FFCM_ERR_ARGUMENT, "per-system arrays must not be NULL");
+    for (int64_t i = 0; i < nsys; ++i) {
+        const int r = ffcm_validate_config(dtype, L + 3 * i, R_c[i], N[i], a, ratio, M + 3 * i, M_G,
+                                           mu, FFCM_FFT_ESTIMATE, 1);
+        if (r != FFCM_OK) return fail(r, "system " + std::to_string(i) + ": " + g_err);
+    }
+    DeviceGuard g(device);
+    if (!g.ok) return fail(FFCM_ERR_CUDA, "cudaSetDevice failed");
+    auto* b = new ffcm_batch();
+    b->dtype = dtype;
+    b->device = device;
+    b->nrhs = nrhs;
+    b->nsys = nsys;
+    b->esize = dtype == FFCM_FLOAT32 ? 4 : 8;
+    auto bail = [&](int code) {
+        const std::string msg = g_err;
+        batch_release(b);
+        return fail(code, msg);
+    };
+    int64_t acc = 0;
+    for (int64_t i = 0; i < nsys; ++i) {
+        ffcm_handle* h = nullptr;
+        const int r = ffcm_create(&h, dtype, L + 3 * i, R_c[i], N[i], a, ratio, M + 3 * i, M_G, mu,
+                                  FFCM_FFT_ESTIMATE, 1, device);
+        if (r != FFCM_OK) return bail(r);
+        b->sys.push_back(h);
+        if (!h->eng->uses_slab()) {
+            const int rr = h->eng->ensure_real_grids();   // before any capture
+            if (rr != FFCM_OK) return bail(rr);
+        }
+        b->N.push_back(N[i]);
+        b->yoff.push_back(acc);
+        b->fvoff.push_back(3 * nrhs * acc);
+        acc += N[i];
+    }
+    b->totalN = acc;
+    const size_t ybytes = 3 * (size_t)acc * b->esize, fvbytes = (size_t)nrhs * ybytes;
+    if (cudaMalloc(&b->Yb, ybytes) != cudaSuccess || cudaMalloc(&b->Fb, fvbytes) != cudaSuccess ||
+        cudaMalloc(&b->Vb, fvbytes) != cudaSuccess) {
+        fail(FFCM_ERR_OOM, "batch staging buffers");
+        return bail(FFCM_ERR_OOM);
+    }
+    if (cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking) != cudaSuccess) {
+        fail(FFCM_ERR_CUDA, "stream creation");
+        return bail(FFCM_ERR_CUDA);
+    }
+    b->ws.resize(nsys, nullptr);
+    b->ev.resize(nsys + 1, nullptr);
+    for (auto& s : b->ws)
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) {
+            fail(FFCM_ERR_CUDA, "stream creation");
+            return bail(FFCM_ERR_CUDA);
+        }
+    for (auto& e : b->ev)
+        if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+            fail(FFCM_ERR_CUDA, "event creation");
+            return bail(FFCM_ERR_CUDA);
+        }
+    const int r = batch_build_graph(b);
+    if (r != FFCM_OK) return bail(r);
+    *out = b;
+    return FFCM_OK;
+}
+
+int ffcm_batch_destroy(ffcm_batch* b) {
+    batch_release(b);
+    return FFCM_OK;
+}
+
+int ffcm_batch_get_info(const ffcm_batch* b, int64_t* total, int64_t* nsys, int32_t* nrhs,
+                        int64_t* kernels) {
+    if (!b) return fail(FFCM_ERR_STATE, "null batch");
+    if (total) *total = b->totalN;
+    if (nsys) *nsys = b->nsys;
+    if (nrhs) *nrhs = b->nrhs;
+    if (kernels) *kernels = b->kernels;
+    return FFCM_OK;
+}
+
+int ffcm_batch_mobility(ffcm_batch* b, void* V, const void* Y, const void* F, int32_t memory,
+                        void* stream) {
+    g_err.clear();
+    if (!b || !b->exec) return fail(FFCM_ERR_STATE, "null or unbuilt batch");
+    TRY(check_memory(memory));
+    if (!V || !Y || !F) return fail(FFCM_ERR_ARGUMENT, "V, Y and F must not be NULL");
+    DeviceGuard g(b->device);
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->main;
+    const size_t ybytes = 3 * (size_t)b->totalN * b->esize, fvbytes = (size_t)b->nrhs * ybytes;
+    CUDA_TRY(cudaMemcpyAsync(b->Yb, Y, ybytes, kind_to_dev(memory), s));
+    CUDA_TRY(cudaMemcpyAsync(b->Fb, F, fvbytes, kind_to_dev(memory), s));
+    CUDA_TRY(cudaGraphLaunch(b->exec, s));
+    for (ffcm_handle* h : b->sys) h->launches += b->kernels / std::max<int64_t>(1, b->nsys);
+    CUDA_TRY(cudaMemcpyAsync(V, b->Vb, fvbytes, kind_from_dev(memory), s));
+    if (memory != FFCM_HOST) return FFCM_OK;
+    for (ffcm_handle* h : b->sys) TRY(finish(h, s));
+    return FFCM_OK;
+}
 
 }  // extern "C"

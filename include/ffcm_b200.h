@@ -19,7 +19,8 @@
  *  - `memory` says whether a pointer is host (FFCM_HOST) or device
  *    (FFCM_DEVICE) memory. Host calls copy through the handle and return after
  *    the result is in host memory; device calls are asynchronous on `stream`.
- *  - `stream` is a cudaStream_t (NULL = the handle's own stream).
+ *  - `stream` is a cudaStream_t: NULL = the handle's own stream; the
+ *    special handles cudaStreamLegacy / cudaStreamPerThread are accepted.
  *  - Index buffers exchanged through ffcm_get_buffer/ffcm_set_buffer are
  *    1-based, as in the reference (`original_index`, `cell_start`,
  *    `cell_end`); cell hashes are 0-based as in the reference.
@@ -179,6 +180,36 @@ int ffcm_set_buffer(ffcm_handle* h, int32_t which, const void* src, int64_t nbyt
 /* Wait for the handle's work on `stream` and report any sticky device-side
  * error (non-finite position, a bounded wait that gave up). */
 int ffcm_synchronize(ffcm_handle* h, void* stream);
+
+/* ---- batched form ---------------------------------------------------------
+ * Many independent suspensions (each one FFCMConfig of the reference), each
+ * with nrhs force right-hand sides, solved by one launch of a CUDA graph
+ * built on the first call. No reference counterpart: the reference solves
+ * one system and one right-hand side per mobility! call; a batch is
+ * equivalent to calling mobility!(V[i][r], config[i], Y[i], F[i][r]) for every
+ * system i and right-hand side r (src/mobility.jl:309-331).
+ *
+ * Shared by all systems: dtype, a, kernel_widths_ratio, M_G, viscosity.
+ * Per system i: L[3i..3i+2], R_c[i], N[i], num_grid_points[3i..3i+2].
+ * Layouts (elements of the handle's type T): system i's positions start at
+ * 3 * sum_{j<i} N[j] of Y; its forces and velocities at
+ * 3 * nrhs * sum_{j<i} N[j] of F and V, right-hand side r at that offset plus
+ * 3 * r * N[i]; each block is the reference's 3xN column-major matrix. */
+typedef struct ffcm_batch ffcm_batch;
+
+int ffcm_batch_create(ffcm_batch** out, int32_t dtype, int64_t nsys, const double* L,
+                      const double* R_c, const int64_t* N, double a, double kernel_widths_ratio,
+                      const int32_t* num_grid_points, int32_t M_G, double viscosity,
+                      int32_t nrhs, int32_t device);
+int ffcm_batch_destroy(ffcm_batch* b);
+/* Solve every system and right-hand side. Host memory: returns with V filled.
+ * Device memory: asynchronous on `stream`. */
+int ffcm_batch_mobility(ffcm_batch* b, void* V, const void* Y, const void* F, int32_t memory,
+                        void* stream);
+/* Totals of a batch: particles over all systems, systems, right-hand sides,
+ * and the kernels one ffcm_batch_mobility launches (graph nodes). */
+int ffcm_batch_get_info(const ffcm_batch* b, int64_t* total_particles, int64_t* nsys,
+                        int32_t* nrhs, int64_t* kernels_per_call);
 
 /* ---- measurement --------------------------------------------------------- */
 

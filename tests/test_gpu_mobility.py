@@ -211,7 +211,11 @@ def test_c2_full_size_against_oracle(ffcm, c2_inputs):
     o64 = O.OracleConfig(np.float64, **kw)
     o64.fft_threads = 8
     V64 = O.apply(o64, Y32.astype(np.float64), F32.astype(np.float64))
-    assert rel_l2(Vg, V64) < 1e-4
+    # The reference's Float32 arithmetic itself sits ~2.2e-4 from Float64 here
+    # (stencil offsets g*h - Y cancel two numbers near L = 275.6); the GPU must
+    # be no less accurate than that algorithm.
+    ref_err = rel_l2(V32, V64)
+    assert rel_l2(Vg, V64) <= max(1e-4, 1.05 * ref_err)
 
 
 def test_c2_full_size_properties(ffcm, c2_inputs):
@@ -238,3 +242,38 @@ def test_c2_full_size_properties(ffcm, c2_inputs):
     assert abs(s1 - s2) <= 1e-4 * np.sqrt(np.sum(F32.astype(np.float64) * VF) *
                                           np.sum(G32.astype(np.float64) * VG))  # symmetry
     assert np.sum(F32.astype(np.float64) * VF) > 0            # positivity
+
+
+# ---- the fused slab path (spread -> x r2c, x c2r -> interpolation) -----------
+@pytest.mark.parametrize("T", TS)
+@pytest.mark.parametrize("L,M,MG,N,R_c", [
+    ((32.0, 4.0, 4.0), (64, 8, 8), 8, 200, 1.0),      # stencil wraps every y/z row
+    ((64.0, 32.0, 16.0), (128, 64, 32), 8, 3000, 2.0),
+    ((40.0, 40.0, 40.0), (64, 64, 64), 6, 2000, 3.0),
+    ((64.0, 64.0, 64.0), (256, 256, 256), 8, 20000, 3.0),
+])
+def test_slab_path_matches_oracle(ffcm, T, L, M, MG, N, R_c):
+    kw = dict(L=L, R_c=R_c, N=N, kernel_widths_ratio=2.0, viscosity=1.0, num_grid_points=M, M_G=MG)
+    prod, ora = both(ffcm, T, **kw)
+    Y, F = random_cloud(T, N, L, 42)
+    Y[0] = np.array(L, T)                  # a particle on the upper boundary
+    Vg = _run(ffcm, prod, Y, F)
+    Vo = O.apply(ora, Y, F)
+    assert np.array_equal(prod.original_index, ora.original_index)
+    assert rel_l2(Vg, Vo) < (1e-5 if T == np.float32 else 1e-11)
+
+
+def test_fused_and_unfused_paths_agree(ffcm, monkeypatch):
+    z = np.load(GOLDEN / "c1_N2000_64.npz")
+    kw = kw_of(40.0, 2000, 64, R_c=3.0)
+    fused = ffcm.FFCMConfig(np.float32, **kw)
+    monkeypatch.setenv("FFCM_NO_SLAB", "1")
+    plain = ffcm.FFCMConfig(np.float32, **kw)
+    monkeypatch.delenv("FFCM_NO_SLAB")
+    Va = _run(ffcm, fused, z["f32_Y"], z["f32_F"])
+    Vb = _run(ffcm, plain, z["f32_Y"], z["f32_F"])
+    assert rel_l2(Va, Vb) < 2e-6
+    # the interpolation of the fused path is deterministic (no atomics)
+    Vc = _run(ffcm, fused, z["f32_Y"], z["f32_F"])
+    Vd = _run(ffcm, fused, z["f32_Y"], z["f32_F"])
+    assert rel_l2(Vc, Vd) < 1e-6
