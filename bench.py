@@ -39,25 +39,44 @@ UNIT = "particles/s"
 WORK = dict(L=275.6, N=500_000, M=512, M_G=8, R_c=3.0, ratio=2.0, mu=1.0, seed=2024 + 1)
 
 
+GRID = None   # optional (Mx, My, Mz) override for small profiling cases
+
+
+def work_geometry():
+    """(L, N, M) of the workload; a --grid override keeps the spacing
+    h = 275.6/512 and the particle density, scaling the box and N."""
+    w = WORK
+    if GRID is None:
+        return (w["L"],) * 3, w["N"], (w["M"],) * 3
+    h = w["L"] / w["M"]
+    L = tuple(h * m for m in GRID)
+    N = int(round(w["N"] * np.prod(GRID) / w["M"] ** 3))
+    return L, N, tuple(GRID)
+
+
 def config_kwargs():
     w = WORK
-    return dict(L=(w["L"],) * 3, R_c=w["R_c"], N=w["N"], kernel_widths_ratio=w["ratio"],
-                viscosity=w["mu"], num_grid_points=(w["M"],) * 3, M_G=w["M_G"])
+    L, N, M = work_geometry()
+    return dict(L=L, R_c=w["R_c"], N=N, kernel_widths_ratio=w["ratio"],
+                viscosity=w["mu"], num_grid_points=M, M_G=w["M_G"])
 
 
 def workload_config():
     w = WORK
-    return {"workload": f"plain FFCM mobility, N={w['N']}, L={w['L']}, grid {w['M']}^3, "
-                        f"M_G={w['M_G']}, R_c={w['R_c']}, Sigma/sigma={w['ratio']}, Float32",
-            "N": w["N"], "grid": [w["M"]] * 3, "M_G": w["M_G"],
+    L, N, M = work_geometry()
+    return {"workload": f"plain FFCM mobility, N={N}, L={L[0] if len(set(L)) == 1 else L}, grid "
+                        f"{M[0] if len(set(M)) == 1 else M}^3, M_G={w['M_G']}, R_c={w['R_c']}, "
+                        f"Sigma/sigma={w['ratio']}, Float32",
+            "N": N, "grid": list(M), "M_G": w["M_G"],
             "l2": "working set ~5 GB >> 126 MB L2 (grids rewritten every step); no flush needed"}
 
 
 def make_inputs():
     from fixtures import nonoverlapping_uniform
     w = WORK
-    Y = nonoverlapping_uniform(w["N"], w["L"], w["seed"]).astype(np.float32)
-    F = np.random.default_rng(w["seed"]).standard_normal((w["N"], 3)).astype(np.float32)
+    L, N, _ = work_geometry()
+    Y = nonoverlapping_uniform(N, L, w["seed"]).astype(np.float32)
+    F = np.random.default_rng(w["seed"]).standard_normal((N, 3)).astype(np.float32)
     return Y, F
 
 
@@ -65,10 +84,10 @@ def algorithmic_bytes(T_bytes=4):
     """Compulsory HBM traffic per solve and per stage (each input read once,
     each output written once)."""
     w = WORK
-    N, M = w["N"], w["M"]
-    grid = 3 * M ** 3 * T_bytes
-    spec = 3 * (M // 2 + 1) * M * M * 2 * T_bytes
-    ncell = int(np.floor(np.float32(w["L"]) / np.float32(w["R_c"]))) ** 3
+    L, N, M3 = work_geometry()
+    grid = 3 * int(np.prod(M3)) * T_bytes
+    spec = 3 * (M3[0] // 2 + 1) * M3[1] * M3[2] * 2 * T_bytes
+    ncell = int(np.prod([max(int(np.floor(np.float32(x) / np.float32(w["R_c"]))), 3) for x in L]))
     per = {
         "cell_list": N * (12 + 12 + 4 + 4 + 24) + 8 * ncell,
         "spread": grid + 24 * N,
@@ -172,28 +191,71 @@ def cpu_baseline_run(Y, F, threads):
 
 
 def run_reference(args, rank, world):
+    """The reference's CPU algorithm (the oracle restatement; Julia is not
+    installed here) on the host cores, on the same workload as --workload."""
     if rank != 0:
         return 0
-    import ffcm_oracle as O  # noqa: F401
-    Y, F = make_inputs()
+    import ffcm_oracle as O
     threads = os.cpu_count() or 1
-    # each step is one full solve (~tens of seconds); bound the run to a few minutes
+    # each step is one full evaluation (seconds to tens of seconds): bound the run
     warm = min(args.warmup, 1)
     steps = min(args.steps, 3)
+    if args.workload == "adjoint":
+        Y, F, Yp = adjoint_inputs()
+        cfg = O.OracleConfig(np.float32, **adjoint_kwargs(), fft_threads=threads)
+        Vt = O.apply(cfg, Yp, F)
+        fn = lambda: cpu_adjoint_run(Y, F, Vt, threads)  # noqa: E731
+        units, unit = Y.shape[0], "particles/s"
+        metric = "particles/s per gradient evaluation (J, dJ/dY, dJ/dF; N=100k, 256^3, Float32)"
+        config = adjoint_config()
+        sample = (f"{warm} warm-up + {steps} timed objective-gradient evaluations of the workload by "
+                  "the C/pocketfft restatement (forward, residual, pullback)")
+    elif args.workload == "batched":
+        from fixtures import nonoverlapping_uniform
+        b = BATCH
+        systems = batched_systems()
+        order = np.argsort([s_["N"] for s_ in systems])
+        pick = [int(order[k]) for k in range(3, len(systems), 8)]  # 8 systems, stratified by N
+        rng = np.random.default_rng(b["seed"] + 1)
+        cases = []
+        for i in pick:
+            s_ = systems[i]
+            cfg = O.OracleConfig(np.float32, L=s_["L"], R_c=s_["R_c"], N=s_["N"],
+                                 num_grid_points=s_["num_grid_points"], kernel_widths_ratio=b["ratio"],
+                                 M_G=b["M_G"], viscosity=b["mu"], fft_threads=threads)
+            y = nonoverlapping_uniform(s_["N"], s_["L"][0], b["seed"] + 10 + i).astype(np.float32)
+            cases.append((cfg, y, rng.standard_normal((s_["N"], 3)).astype(np.float32)))
+
+        def fn():
+            t0 = time.perf_counter()
+            for cfg, y, f in cases:
+                O.apply(cfg, y, f)
+            return time.perf_counter() - t0
+
+        units, unit = len(cases), "solves/s"
+        metric = f"solves/s, batched form ({b['nsys']} systems x {b['nrhs']} right-hand sides)"
+        config = {"workload": "batched FFCM mobility (see the ours line); reference solves systems "
+                              "one at a time", "total_particles": int(sum(s_["N"] for s_ in systems))}
+        sample = (f"{warm} warm-up + {steps} timed passes over 8 of the 64 systems (stratified by N), "
+                  "one right-hand side each, by the C/pocketfft restatement; solves/s of that sample")
+    else:
+        Y, F = make_inputs()
+        fn = lambda: cpu_baseline_run(Y, F, threads)  # noqa: E731
+        units, unit, metric, config = Y.shape[0], UNIT, METRIC, workload_config()
+        sample = (f"{warm} warm-up + {steps} timed full solves of the workload by the C/pocketfft "
+                  f"restatement of the reference CPU path (Julia is not installed)")
     for _ in range(warm):
-        cpu_baseline_run(Y, F, threads)
-    ts = [cpu_baseline_run(Y, F, threads) for _ in range(steps)]
+        fn()
+    ts = [fn() for _ in range(steps)]
     sec = float(np.mean(ts))
-    value = WORK["N"] / sec
-    sample = (f"{warm} warm-up + {steps} timed full solves of the workload by the C/pocketfft "
-              f"restatement of the reference CPU path (Julia is not installed)")
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+    value = units / sec
+    line = {"impl": "reference", "metric": metric, "value": value, "unit": unit, "n_gpus": world,
             "steps": steps, "warmup": warm, "ms_per_step": sec * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+            "config": config,
+            "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
                              "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -219,7 +281,7 @@ def run_ours(args, rank, world, local_rank):
                                 device_id=dev)
 
     Y, F = make_inputs()
-    N = WORK["N"]
+    N = Y.shape[0]
     cfg = ffcm.FFCMConfig(np.float32, device=local_rank, **config_kwargs())
     Yd = torch.from_numpy(Y).to(dev)
     Fd = torch.from_numpy(F).to(dev)
@@ -331,6 +393,327 @@ def run_ours(args, rank, world, local_rank):
     return 0
 
 
+BATCH = dict(nsys=64, nrhs=16, Nmin=2000, Nmax=64000, phi=0.1, h0=0.54, Mmin=64, Mmax=256,
+             R_c=3.0, M_G=8, ratio=2.0, mu=1.0, seed=2024 + 2)
+
+
+def batched_systems():
+    """64 suspensions: N log-uniform in [2k, 64k], cubic box at 10% volume
+    fraction, grid the power of two nearest (in log) to L / 0.54, clamped to
+    [64, 256]."""
+    b = BATCH
+    rng = np.random.default_rng(b["seed"])
+    Ns = np.exp(rng.uniform(np.log(b["Nmin"]), np.log(b["Nmax"]), b["nsys"])).astype(np.int64)
+    out = []
+    for n in Ns:
+        L = float((n * 4.0 * np.pi / 3.0 / b["phi"]) ** (1.0 / 3.0))
+        M = int(2 ** int(np.round(np.log2(L / b["h0"]))))
+        M = min(b["Mmax"], max(b["Mmin"], M))
+        out.append(dict(L=(L, L, L), R_c=b["R_c"], N=int(n), num_grid_points=(M, M, M)))
+    return out
+
+
+def shard_systems(systems, world):
+    """Greedy longest-processing-time assignment of systems to ranks by a cost
+    model (particles x stencil + grid x log grid)."""
+    cost = [s["N"] * 512 + 3 * np.prod(s["num_grid_points"]) * np.log2(np.prod(s["num_grid_points"]))
+            for s in systems]
+    order = np.argsort(cost)[::-1]
+    load = [0.0] * world
+    owner = [0] * len(systems)
+    for i in order:
+        r = int(np.argmin(load))
+        owner[i] = r
+        load[r] += cost[i]
+    return owner
+
+
+def run_batched(args, rank, world, local_rank):
+    import torch
+    import importlib.util
+    from fixtures import nonoverlapping_uniform
+
+    pkg = ROOT / "ffcm.jl_b200"
+    spec = importlib.util.spec_from_file_location("ffcm_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    ffcm = importlib.util.module_from_spec(spec)
+    sys.modules["ffcm_b200"] = ffcm
+    spec.loader.exec_module(ffcm)
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    b = BATCH
+    systems_all = batched_systems()
+    owner = shard_systems(systems_all, world)
+    mine = [i for i in range(len(systems_all)) if owner[i] == rank]
+    systems = [systems_all[i] for i in mine]
+    rng = np.random.default_rng(b["seed"] + 1)
+    Ys = [nonoverlapping_uniform(s["N"], s["L"][0], b["seed"] + 10 + i).astype(np.float32)
+          for i, s in zip(mine, systems)]
+    Fs = [[rng.standard_normal((s["N"], 3)).astype(np.float32) for _ in range(b["nrhs"])]
+          for s in systems]
+    common = dict(kernel_widths_ratio=b["ratio"], M_G=b["M_G"], viscosity=b["mu"])
+    batch = ffcm.FFCMBatch(np.float32, systems=systems, nrhs=b["nrhs"], device=local_rank, **common)
+    Yf, Ff = batch.pack(Ys, Fs)
+    Yd, Fd = torch.from_numpy(Yf).to(dev), torch.from_numpy(Ff).to(dev)
+    Vd = torch.empty_like(Fd)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize(dev)
+
+    def timed(fn, steps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
+    for _ in range(args.warmup):
+        batch.mobility(Vd, Yd, Fd)
+    with ClockSampler(local_rank) as clk:
+        ms_batch = timed(lambda: batch.mobility(Vd, Yd, Fd), args.steps)
+    # the same solves through the plain single-system path, called sequentially
+    cfgs = [ffcm.FFCMConfig(np.float32, L=s["L"], R_c=s["R_c"], N=s["N"],
+                            num_grid_points=s["num_grid_points"], device=local_rank, **common)
+            for s in systems]
+    views = []
+    for i, s in enumerate(systems):
+        y = Yd[batch.yoff[i]: batch.yoff[i] + s["N"]]
+        for r in range(b["nrhs"]):
+            o = batch.fvoff[i] + r * s["N"]
+            views.append((cfgs[i], y, Fd[o: o + s["N"]], Vd[o: o + s["N"]]))
+
+    def plain_loop():
+        for cfg, y, f, v in views:
+            ffcm.mobility(v, cfg, y, f)
+
+    plain_loop()
+    ms_plain = timed(plain_loop, max(1, args.steps // 4))
+    # end to end with pinned host buffers
+    Yh = torch.from_numpy(Yf).pin_memory()
+    Fh = torch.from_numpy(Ff).pin_memory()
+    Vh = torch.empty_like(Fh).pin_memory()
+    batch.mobility(Vh, Yh, Fh, stream=stream)
+    ms_e2e = timed(lambda: batch.mobility(Vh, Yh, Fh, stream=stream), args.steps)
+    if dist is not None:
+        t = torch.tensor([ms_batch, ms_plain, ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_batch, ms_plain, ms_e2e = (float(x) for x in t)
+    if rank == 0:
+        solves = b["nsys"] * b["nrhs"]
+        grids = sorted(set(s["num_grid_points"][0] for s in systems_all))
+        line = {
+            "metric": f"solves/s, batched form ({b['nsys']} systems x {b['nrhs']} right-hand sides)",
+            "value": solves / (ms_batch / 1e3), "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_batch,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "batched FFCM mobility: 64 suspensions, N log-uniform in [2000, "
+                                   "64000], 10% volume fraction, grids " + "/".join(f"{g}^3" for g in grids)
+                                   + ", 16 right-hand sides each, M_G=8, R_c=3, Sigma/sigma=2",
+                       "total_particles": int(sum(s["N"] for s in systems_all)),
+                       "parallelism": "systems sharded across ranks" if world > 1 else "single"},
+            "plain_looped": {"value": solves / (ms_plain / 1e3), "unit": "solves/s", "ms": ms_plain,
+                             "how": "ffcm_mobility per (system, right-hand side), device arrays, "
+                                    "one stream"},
+            "speedup_vs_plain_looped": ms_plain / ms_batch,
+            "e2e": {"value": solves / (ms_e2e / 1e3), "unit": "solves/s", "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": int(Yh.numel() * 4 + Fh.numel() * 4),
+                    "d2h_bytes_per_step": int(Vh.numel() * 4)},
+            "clocks": clk.summary(),
+            "gpu_launches": int(batch.kernels_per_call * args.steps),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for c in cfgs:
+        c.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+ADJ = dict(L=161.0, N=100_000, M=256, M_G=8, R_c=3.0, ratio=2.0, mu=1.0, perturb=0.05,
+           seed=2024 + 4)
+
+
+def adjoint_kwargs():
+    a = ADJ
+    return dict(L=(a["L"],) * 3, R_c=a["R_c"], N=a["N"], kernel_widths_ratio=a["ratio"],
+                viscosity=a["mu"], num_grid_points=(a["M"],) * 3, M_G=a["M_G"])
+
+
+def adjoint_config():
+    a = ADJ
+    return {"workload": f"adjoint FFCM: J = 0.5 |V(Y, F) - V_t|^2 with dJ/dY and dJ/dF, N={a['N']}, "
+                        f"L={a['L']}, grid {a['M']}^3, M_G={a['M_G']}, R_c={a['R_c']}, "
+                        f"Sigma/sigma={a['ratio']}, V_t = V at Y + N(0, {a['perturb']}^2), Float32",
+            "N": a["N"], "grid": [a["M"]] * 3, "M_G": a["M_G"],
+            "l2": "working set ~1 GB (spectrum + u and psi grids) >> 126 MB L2; no flush needed"}
+
+
+def adjoint_inputs():
+    from fixtures import nonoverlapping_uniform
+    a = ADJ
+    Y = nonoverlapping_uniform(a["N"], a["L"], a["seed"])
+    rng = np.random.default_rng(a["seed"])
+    F = rng.standard_normal((a["N"], 3))
+    Yp = Y + rng.normal(0.0, a["perturb"], Y.shape)
+    return Y.astype(np.float32), F.astype(np.float32), Yp.astype(np.float32)
+
+
+def adjoint_bytes(T_bytes=4):
+    """Compulsory HBM traffic per stage of the pullback (see algorithmic_bytes)."""
+    a = ADJ
+    N, M = a["N"], a["M"]
+    grid = 3 * M ** 3 * T_bytes
+    spec = 3 * (M // 2 + 1) * M * M * 2 * T_bytes
+    return {"cell_list": 12 * N + 16 * N + 4 * N,
+            "spread": grid + 32 * N,
+            "fft_y_fwd": 2 * spec, "fft_z_stokes": 2 * spec, "fft_y_inv": 2 * spec,
+            "fft_x_inv": spec + grid,
+            "interpolate": 2 * grid + 3 * 16 * N + 4 * N + 24 * N,
+            "correct": 3 * 16 * N + 4 * N + 2 * 2 * 12 * N}
+
+
+def run_adjoint(args, rank, world, local_rank):
+    import torch
+    ffcm = _load_product()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    Y, F, Yp = adjoint_inputs()
+    N = Y.shape[0]
+    cfg = ffcm.FFCMConfig(np.float32, device=local_rank, **adjoint_kwargs())
+    Yd, Fd = torch.from_numpy(Y).to(dev), torch.from_numpy(F).to(dev)
+    Vt = torch.empty_like(Yd)
+    ffcm.mobility(Vt, cfg, torch.from_numpy(Yp).to(dev), Fd)
+    V, dY, dF = (torch.empty_like(Yd) for _ in range(3))
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize(dev)
+
+    def timed(fn, steps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
+    def grad_step():
+        ffcm.objective_gradient(cfg, Yd, Fd, Vt, V=V, dY=dY, dF=dF)
+
+    for _ in range(args.warmup):
+        grad_step()
+    launches0 = cfg.launch_count()
+    with ClockSampler(local_rank) as clk:
+        ms_grad = timed(grad_step, args.steps)
+    launches = cfg.launch_count() - launches0
+    ms_fwd = timed(lambda: ffcm.mobility(V, cfg, Yd, Fd), args.steps)
+    ffcm.mobility_checkpoint(V, cfg, Yd, Fd)
+    ms_ckpt = timed(lambda: ffcm.mobility_checkpoint(V, cfg, Yd, Fd), args.steps)
+    lam = (V - Vt).contiguous()
+    ms_pull = timed(lambda: ffcm.adjoint(dY, dF, cfg, lam), args.steps)
+    cfg.profile_begin()
+    for _ in range(args.steps):
+        ffcm.adjoint(dY, dF, cfg, lam)
+    torch.cuda.synchronize(dev)
+    stages = cfg.profile_end()
+    # end to end: host arrays in, V, dJ/dY, dJ/dF and J out, every step
+    Yh, Fh, Th = (torch.from_numpy(a).pin_memory() for a in (Y, F, Vt.cpu().numpy()))
+    Vh, dYh, dFh = (torch.empty_like(Yh).pin_memory() for _ in range(3))
+    ffcm.objective_gradient(cfg, Yh, Fh, Th, V=Vh, dY=dYh, dF=dFh, stream=stream)
+    ms_e2e = timed(lambda: ffcm.objective_gradient(cfg, Yh, Fh, Th, V=Vh, dY=dYh, dF=dFh, stream=stream),
+                   args.steps)
+    if dist is not None:
+        t = torch.tensor([ms_grad, ms_fwd, ms_pull, ms_ckpt, ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_grad, ms_fwd, ms_pull, ms_ckpt, ms_e2e = (float(x) for x in t)
+    if rank == 0:
+        per = adjoint_bytes()
+        peak, peak_kind = measured_peak_hbm()
+        stage_ms = {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1] > 0}
+        ks = [k for k in per if k in stage_ms]
+        dom = max(ks, key=lambda k: stage_ms[k])
+        achieved = per[dom] / (stage_ms[dom] / 1e3) / 1e9
+        cpu = None
+        if not args.skip_cpu_baseline:
+            sec = cpu_adjoint_run(Y, F, Vt.cpu().numpy(), os.cpu_count() or 1)
+            cpu = {"value": N / sec, "unit": "particles/s", "cores": os.cpu_count() or 1, "kind": "port",
+                   "sample": "one objective-gradient evaluation of the workload by the C/pocketfft "
+                             "oracle (forward, residual, pullback)"}
+        line = {
+            "metric": "particles/s per gradient evaluation (J, dJ/dY, dJ/dF; N=100k, 256^3, Float32)",
+            "value": world * N / (ms_grad / 1e3), "unit": "particles/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_grad,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {**adjoint_config(), "parallelism": "replicas" if world > 1 else "single"},
+            "forward_ms": ms_fwd, "checkpointed_forward_ms": ms_ckpt, "pullback_ms": ms_pull,
+            "pullback_cost_vs_forward": ms_pull / ms_fwd,
+            "gradient_step_cost_vs_forward": ms_grad / ms_fwd,
+            "e2e": {"value": world * N / (ms_e2e / 1e3), "unit": "particles/s", "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": int(3 * Yh.numel() * 4),
+                    "d2h_bytes_per_step": int(3 * Yh.numel() * 4 + 8)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": None,
+                         "algorithmic_bytes_per_launch": per[dom]},
+            "pullback_stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    cfg.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_adjoint_run(Y, F, Vt, threads):
+    import ffcm_oracle as O
+    cfg = O.OracleConfig(np.float32, **adjoint_kwargs(), fft_threads=threads)
+    t0 = time.perf_counter()
+    O.objective_gradient(cfg, Y, F, Vt)
+    return time.perf_counter() - t0
+
+
+def _load_product():
+    import importlib.util
+    if "ffcm_b200" in sys.modules:
+        return sys.modules["ffcm_b200"]
+    pkg = ROOT / "ffcm.jl_b200"
+    spec = importlib.util.spec_from_file_location("ffcm_b200", pkg / "__init__.py",
+                                                  submodule_search_locations=[str(pkg)])
+    ffcm = importlib.util.module_from_spec(spec)
+    sys.modules["ffcm_b200"] = ffcm
+    spec.loader.exec_module(ffcm)
+    return ffcm
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -338,7 +721,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["plain", "batched", "adjoint"], default="plain")
+    ap.add_argument("--grid", default=None,
+                    help="Mx,My,Mz: smaller case at the same spacing and density (profiling)")
     args = ap.parse_args()
+    global GRID
+    if args.grid:
+        GRID = tuple(int(x) for x in args.grid.split(","))
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     rank = int(os.environ.get("RANK", 0))
@@ -346,6 +735,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "batched":
+        return run_batched(args, rank, world, local_rank)
+    if args.workload == "adjoint":
+        return run_adjoint(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

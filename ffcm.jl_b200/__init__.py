@@ -32,9 +32,11 @@ import numpy as np
 
 from . import _lib as L_
 
-__all__ = ["FFCMConfig", "mobility", "FFCMMobility", "ArgumentError", "DimensionMismatch",
+__all__ = ["FFCMConfig", "mobility", "FFCMMobility", "FFCMBatch", "ArgumentError", "DimensionMismatch",
            "FFCMError", "wrap_positions", "assign_cells", "sort_particles_by_cell",
-           "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities"]
+           "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities",
+           "mobility_checkpoint", "adjoint", "objective_gradient", "rrule_mobility",
+           "mobility_autograd"]
 
 
 class ArgumentError(ValueError):
@@ -432,6 +434,124 @@ class FFCMMobility:
         return True
 
 
+# ---- adjoint form (no reference counterpart: the reference has no derivative) ----
+
+def _particle_args(config, named, writable=()):
+    """_Arg per (name, array); all 3xN of the config's N, one memory kind."""
+    T = config.T
+    args = []
+    for name, x in named:
+        if len(getattr(x, "shape", ())) != 2:
+            raise DimensionMismatch(f"{name} must be 3xN for the config's N = {config.N}")
+        a = _Arg(x, T, writable=name in writable)
+        if (a.rows, a.cols) != (3, config.N):
+            raise DimensionMismatch(f"{name} must be 3xN for the config's N = {config.N}; "
+                                    f"got size ({a.rows}, {a.cols})")
+        args.append(a)
+    if len({a.memory for a in args}) != 1:
+        raise ArgumentError("all arrays must be host arrays or all be CUDA tensors")
+    return args
+
+
+def mobility_checkpoint(V, config: FFCMConfig, Y, F, stream=None):
+    """``mobility!`` that also keeps what the pullback needs (the velocity grid
+    u = L^-1 S F, the cell list and the sorted particles) on the config."""
+    v, y, f = _particle_args(config, (("V", V), ("Y", Y), ("F", F)), writable=("V",))
+    st = _stream_of(v) if stream is None else _stream_handle(stream)
+    _raise(L_.load().ffcm_mobility_checkpoint(config.handle, v.ptr, y.ptr, f.ptr, v.memory, st))
+    return V
+
+
+def adjoint(dY, dF, config: FFCMConfig, lam, stream=None):
+    """Pullback of the last ``mobility_checkpoint`` on ``config`` at the
+    cotangent ``lam`` = dJ/dV: writes dJ/dY into ``dY`` and dJ/dF = M lam into
+    ``dF`` (3xN each). Raises FFCMError if another solve ran since."""
+    gy, gf, l_ = _particle_args(config, (("dY", dY), ("dF", dF), ("lambda", lam)),
+                                writable=("dY", "dF"))
+    st = _stream_of(gy) if stream is None else _stream_handle(stream)
+    _raise(L_.load().ffcm_adjoint(config.handle, gy.ptr, gf.ptr, l_.ptr, gy.memory, st))
+    return dY, dF
+
+
+def objective_gradient(config: FFCMConfig, Y, F, V_target, *, V=None, dY=None, dF=None, stream=None):
+    """J = 0.5 |M(Y) F - V_target|^2 with its gradients, in one call.
+
+    Returns ``(J, dJ/dY, dJ/dF, V)``. Host arrays give a float J; CUDA tensors
+    give J as a one-element float64 CUDA tensor (the call stays asynchronous).
+    """
+    T = config.T
+    dev = _is_torch(Y) and Y.is_cuda
+    if dev:
+        import torch
+        mk = lambda: torch.empty_like(Y)  # noqa: E731
+        Jbuf = torch.zeros(1, dtype=torch.float64, device=Y.device)
+        jptr = ctypes.cast(ctypes.c_void_p(Jbuf.data_ptr()), ctypes.POINTER(ctypes.c_double))
+    else:
+        mk = lambda: np.empty((config.N, 3), T)  # noqa: E731
+        Jbuf = ctypes.c_double(0.0)
+        jptr = ctypes.pointer(Jbuf)
+    V = mk() if V is None else V
+    dY = mk() if dY is None else dY
+    dF = mk() if dF is None else dF
+    gy, gf, v, y, f, t = _particle_args(
+        config, (("dY", dY), ("dF", dF), ("V", V), ("Y", Y), ("F", F), ("V_target", V_target)),
+        writable=("dY", "dF", "V"))
+    st = _stream_of(v) if stream is None else _stream_handle(stream)
+    _raise(L_.load().ffcm_objective_gradient(config.handle, jptr, gy.ptr, gf.ptr, v.ptr, y.ptr, f.ptr,
+                                             t.ptr, v.memory, st))
+    return (Jbuf if dev else Jbuf.value), dY, dF, V
+
+
+def rrule_mobility(config: FFCMConfig, Y, F):
+    """Counterpart of a ChainRulesCore ``rrule`` for ``V = mobility(config, Y, F)``:
+    returns ``(V, pullback)`` with ``pullback(Vbar) -> (Ybar, Fbar)``.
+
+    The pullback is valid until the next solve on ``config``.
+    """
+    dev = _is_torch(Y) and Y.is_cuda
+    if dev:
+        import torch
+        mk = lambda: torch.empty_like(Y)  # noqa: E731
+    else:
+        mk = lambda: np.empty((config.N, 3), config.T)  # noqa: E731
+    V = mobility_checkpoint(mk(), config, Y, F)
+
+    def pullback(Vbar):
+        dY, dF = mk(), mk()
+        adjoint(dY, dF, config, Vbar)
+        return dY, dF
+
+    return V, pullback
+
+
+def _torch_function():
+    import torch
+
+    class MobilityFunction(torch.autograd.Function):
+        """``V = M(Y) F`` on CUDA tensors with the hand-written pullback."""
+
+        @staticmethod
+        def forward(ctx, Y, F, config):
+            V = torch.empty_like(Y)
+            mobility_checkpoint(V, config, Y.detach().contiguous(), F.detach().contiguous())
+            ctx.config = config
+            return V
+
+        @staticmethod
+        def backward(ctx, Vbar):
+            dY = torch.empty_like(Vbar)
+            dF = torch.empty_like(Vbar)
+            adjoint(dY, dF, ctx.config, Vbar.contiguous())
+            return dY, dF, None
+
+    return MobilityFunction
+
+
+def mobility_autograd(config: FFCMConfig, Y, F):
+    """Differentiable ``V = M(Y) F`` for CUDA tensors (torch.autograd)."""
+    return _torch_function().apply(Y, F, config)
+
+
 def validate_config(T, *, L, R_c, N, a=1.0, kernel_widths_ratio, num_grid_points, M_G,
                     viscosity, fft_planning="measure", fft_threads=1):
     """Host-only validation (no device work): raises as FFCMConfig would."""
@@ -458,3 +578,91 @@ def derive_scalars(T, *, L, R_c, a=1.0, kernel_widths_ratio, num_grid_points):
     return dict(num_cells=tuple(int(v) for v in nc), cell_size=tuple(T_(v) for v in cs),
                 inv_cell_size=tuple(T_(v) for v in ics), sigma=T_(s.value), Sigma=T_(S.value),
                 h=T_(hh.value), inv_h=T_(ih.value))
+
+
+class FFCMBatch:
+    """Batched form: ``nsys`` independent suspensions, each with ``nrhs`` force
+    right-hand sides, solved by one CUDA-graph launch per call.
+
+    Equivalent to ``mobility(V[i][r], FFCMConfig(systems[i]...), Y[i], F[i][r])``
+    for every system i and right-hand side r. ``systems`` is a list of dicts
+    with ``L``, ``R_c``, ``N``, ``num_grid_points``; the kernel widths ratio,
+    ``M_G``, viscosity and ``a`` are shared. Arrays are flat: system i's
+    positions are rows ``yoff[i]:yoff[i]+N[i]`` of an ``(sum N, 3)`` array and
+    its right-hand side r is rows ``fvoff[i] + r*N[i] : ... + N[i]`` of an
+    ``(nrhs * sum N, 3)`` array (see ``pack``/``unpack``).
+    """
+
+    def __init__(self, T=np.float32, *, systems, kernel_widths_ratio, M_G, viscosity, nrhs=1,
+                 a=1.0, device=0):
+        self._b = None
+        self.T = np.dtype(T).type
+        dt = _dtype_code(T)
+        n = len(systems)
+        if n < 1:
+            raise ArgumentError("a batch needs at least one system")
+        Ls = [float(x) for s_ in systems for x in s_["L"]]
+        Rc = [float(s_["R_c"]) for s_ in systems]
+        Ns = [int(s_["N"]) for s_ in systems]
+        Ms = [int(m) for s_ in systems for m in s_["num_grid_points"]]
+        b = ctypes.c_void_p()
+        _raise(L_.load().ffcm_batch_create(
+            ctypes.byref(b), dt, n, _dptr(Ls), _dptr(Rc), (ctypes.c_int64 * n)(*Ns), float(a),
+            float(kernel_widths_ratio), _i32ptr(Ms), int(M_G), float(viscosity), int(nrhs),
+            int(device)))
+        self._b = b
+        self.N = Ns
+        self.nrhs = int(nrhs)
+        self.nsys = n
+        self.yoff = np.concatenate([[0], np.cumsum(Ns)[:-1]]).astype(np.int64)
+        self.fvoff = self.nrhs * self.yoff
+        total, ns, nr, kern = (ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32(),
+                               ctypes.c_int64())
+        _raise(L_.load().ffcm_batch_get_info(b, ctypes.byref(total), ctypes.byref(ns),
+                                             ctypes.byref(nr), ctypes.byref(kern)))
+        self.total_particles = int(total.value)
+        self.kernels_per_call = int(kern.value)
+
+    def close(self):
+        if getattr(self, "_b", None):
+            L_.load().ffcm_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def pack(self, Ys=None, Fs=None):
+        """Flatten per-system positions [(N_i,3)] and forces [[(N_i,3)] * nrhs]."""
+        out = []
+        if Ys is not None:
+            out.append(np.ascontiguousarray(np.concatenate(
+                [np.asarray(y, self.T).reshape(-1, 3) for y in Ys]), self.T))
+        if Fs is not None:
+            out.append(np.ascontiguousarray(np.concatenate(
+                [np.asarray(f, self.T).reshape(-1, 3) for fr in Fs for f in fr]), self.T))
+        return out[0] if len(out) == 1 else tuple(out)
+
+    def unpack(self, V):
+        """Split a flat velocity array into [[(N_i,3)] * nrhs] per system."""
+        V = np.asarray(V)
+        return [[V[self.fvoff[i] + r * n: self.fvoff[i] + (r + 1) * n] for r in range(self.nrhs)]
+                for i, n in enumerate(self.N)]
+
+    def mobility(self, V, Y, F, stream=None):
+        T = self.T
+        tot = self.total_particles
+        v = _Arg(V, T, writable=True)
+        y = _Arg(Y, T)
+        f = _Arg(F, T)
+        if (y.rows, y.cols) != (3, tot) or (f.rows, f.cols) != (3, tot * self.nrhs) or \
+                (v.rows, v.cols) != (3, tot * self.nrhs):
+            raise DimensionMismatch("batch arrays must be (sum N, 3) for Y and "
+                                    "(nrhs * sum N, 3) for F and V")
+        if len({v.memory, y.memory, f.memory}) != 1:
+            raise ArgumentError("V, Y and F must all be host arrays or all be CUDA tensors")
+        st = _stream_of(v) if stream is None else _stream_handle(stream)
+        _raise(L_.load().ffcm_batch_mobility(self._b, v.ptr, y.ptr, f.ptr, v.memory, st))
+        return V

@@ -74,6 +74,14 @@ SIGNATURES = {
     "ffcm_profile_begin": (_c.c_int, [_vp]),
     "ffcm_profile_end": (_c.c_int, [_vp, _dp, _i64p]),
     "ffcm_launch_count": (_i64, [_vp]),
+    "ffcm_batch_create": (_c.c_int, [_c.POINTER(_vp), _i32, _i64, _dp, _dp, _i64p, _d, _d, _i32p,
+                                     _i32, _d, _i32, _i32]),
+    "ffcm_batch_destroy": (_c.c_int, [_vp]),
+    "ffcm_batch_mobility": (_c.c_int, [_vp, _vp, _vp, _vp, _i32, _vp]),
+    "ffcm_batch_get_info": (_c.c_int, [_vp, _i64p, _i64p, _i32p, _i64p]),
+    "ffcm_mobility_checkpoint": (_c.c_int, [_vp, _vp, _vp, _vp, _i32, _vp]),
+    "ffcm_adjoint": (_c.c_int, [_vp, _vp, _vp, _vp, _i32, _vp]),
+    "ffcm_objective_gradient": (_c.c_int, [_vp, _dp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
 }
 
 _lib = None

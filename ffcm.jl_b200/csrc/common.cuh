@@ -57,6 +57,8 @@ __device__ __forceinline__ float rint_t(float a) { return rintf(a); }
 __device__ __forceinline__ double rint_t(double a) { return rint(a); }
 __device__ __forceinline__ float floor_t(float a) { return floorf(a); }
 __device__ __forceinline__ double floor_t(double a) { return floor(a); }
+__device__ __forceinline__ float fma_t(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_t(double a, double b, double c) { return __fma_rn(a, b, c); }
 __device__ __forceinline__ float exp_t(float a) { return expf(a); }
 __device__ __forceinline__ double exp_t(double a) { return exp(a); }
 __device__ __forceinline__ float erf_t(float a) { return erff(a); }

@@ -8,7 +8,9 @@
 #include <cstring>
 #include <cstdlib>
 #include <functional>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -16,6 +18,7 @@
 #include "common.cuh"
 #include "cell_list.cuh"
 #include "correct.cuh"
+#include "adjoint.cuh"
 #include "fft.cuh"
 #include "fft_dispatch.cuh"
 #include "fft_pipe.cuh"
@@ -49,6 +52,23 @@ int cuda_fail(cudaError_t e, const char* what) {
         int r_ = (expr);            \
         if (r_ != FFCM_OK) return r_; \
     } while (0)
+
+// Raise a kernel's dynamic shared-memory cap to at least `bytes` on the
+// current device. The cap is a property of the function in the process, not
+// of a handle, so it only ever grows: several configurations of different
+// sizes alive at once each keep what they need.
+int raise_smem_cap(const void* func, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> cap;
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    size_t& cur = cap[{dev, func}];
+    if (bytes <= cur) return FFCM_OK;
+    CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+    return FFCM_OK;
+}
 
 std::string fmt(double v) {
     char b[64];
@@ -191,6 +211,11 @@ struct EngineBase {
     virtual int correct(void* V, cudaStream_t s) = 0;
     virtual int mobility_rest(void* V, cudaStream_t s) = 0;
     virtual int gather_forces(const void* F, cudaStream_t s) = 0;
+    virtual int forward_checkpoint(void* V, cudaStream_t s) = 0;
+    virtual int adjoint(const void* lam, void* dY, void* dF, cudaStream_t s) = 0;
+    virtual int residual(const void* V, const void* Vt, void* lam, double* J, cudaStream_t s) = 0;
+    virtual int ensure_adjoint() = 0;
+    virtual void* adj_buf(int which) = 0;  // 0 lambda, 1 dY, 2 dF, 3 target, 4 J (double)
     virtual int ensure_real_grids() = 0;
     virtual bool uses_slab() const = 0;
     virtual void* Y_in() = 0;
@@ -213,6 +238,9 @@ struct ffcm_handle {
     int* d_err = nullptr;
     int* h_err = nullptr;
     int64_t launches = 0;
+    // true while the state of the last ffcm_mobility_checkpoint (cell list,
+    // sorted Y/F, velocity grid) is intact for ffcm_adjoint
+    bool ckpt = false;
     // profiling
     bool profiling = false;
     std::vector<cudaEvent_t> events;
@@ -302,6 +330,12 @@ struct Engine final : EngineBase {
     int32_t* scratch_i = nullptr;
     vec4<T>*Ys = nullptr, *Fs = nullptr;
     T *gf = nullptr, *gu = nullptr;
+    // adjoint state (allocated on first use): sorted cotangent, the adjoint
+    // velocity grid psi, host-staging buffers and the objective accumulator
+    vec4<T>* Ls = nullptr;
+    T *gpsi = nullptr, *Lin = nullptr, *dYo = nullptr, *dFo = nullptr, *Vt = nullptr;
+    double* Jd = nullptr;
+    CorrGradConsts<T> cgc;
     cplx<T>* spec = nullptr;
     cplx<T>*twx = nullptr, *twy = nullptr, *twz = nullptr;
     T *kxv = nullptr, *kyv = nullptr, *kzv = nullptr;
@@ -387,6 +421,10 @@ struct Engine final : EngineBase {
         cc.Rc2 = R * R;
         cc.ic0 = d.inv_cell_size[0]; cc.ic1 = d.inv_cell_size[1]; cc.ic2 = d.inv_cell_size[2];
         cc.m0 = m0; cc.m1 = m1; cc.m2 = m2;
+        cgc.e_s = T(1) / (d.sigma * std::sqrt(pi));
+        cgc.e_S = T(1) / (d.Sigma * std::sqrt(pi));
+        cgc.ds_s = T(1) / (T(2) * s2);
+        cgc.ds_S = T(1) / (T(2) * S2);
 
         // FFT plans and launch shapes
         const bool xeven = (Mx % 2) == 0;
@@ -410,8 +448,8 @@ struct Engine final : EngineBase {
         if (fast_x) {
             lpb_fx = FastFft<T>::x_lpb(Mx / 2);
             smem_fx = FastFft<T>::x_smem(Mx / 2);
-            CUDA_TRY(cudaFuncSetAttribute(xf_kernel<T>(Mx / 2), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fx));
-            CUDA_TRY(cudaFuncSetAttribute(xi_kernel<T>(Mx / 2), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_fx));
+            TRY(raise_smem_cap((const void*)xf_kernel<T>(Mx / 2), smem_fx));
+            TRY(raise_smem_cap((const void*)xi_kernel<T>(Mx / 2), smem_fx));
         }
         auto max_cell_rows = [&](int B, double cs) {
             const double span = (double)(B + MG - 1 + 1) * (double)d.h + 2e-3 * (double)d.h;
@@ -433,23 +471,21 @@ struct Engine final : EngineBase {
             const double expect = (double)N * (sk.BY + MG - 1) * (sk.BZ + MG - 1) / ((double)My * Mz);
             sg.lcap = (int)std::min<double>(1 << 20, std::max(256.0, 4.0 * expect + 64.0));
             sg.lcap = (sg.lcap + 31) / 32 * 32;
-            CUDA_TRY(cudaFuncSetAttribute(sk.spread_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sk.smem));
-            CUDA_TRY(cudaFuncSetAttribute(sk.interp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sk.smem));
+            TRY(raise_smem_cap((const void*)sk.spread_fused, sk.smem));
+            TRY(raise_smem_cap((const void*)sk.interp, sk.smem));
         }
         if (fast_y) {
             int cand[4];
             const int nc = y_bundles(My, cand);
             for (int i = 0; i < nc; ++i)
-                CUDA_TRY(cudaFuncSetAttribute(y_kernel<T>(My, cand[i]), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)FastFft<T>::yz_smem(My, cand[i])));
+                TRY(raise_smem_cap((const void*)y_kernel<T>(My, cand[i]), FastFft<T>::yz_smem(My, cand[i])));
             By = cand[nc - 1];
         }
         if (fast_z) {
             int cand[4];
             const int nc = z_bundles(Mz, cand);
             for (int i = 0; i < nc; ++i)
-                CUDA_TRY(cudaFuncSetAttribute(z_kernel<T>(Mz, cand[i]), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)FastFft<T>::yz_smem(Mz, cand[i])));
+                TRY(raise_smem_cap((const void*)z_kernel<T>(Mz, cand[i]), FastFft<T>::yz_smem(Mz, cand[i])));
             Bz = cand[nc - 1];
         }
         {
@@ -459,19 +495,18 @@ struct Engine final : EngineBase {
         }
         for (int B : {2, 4, 8, 16}) {
             if (fast_y && ypipe_kernel<T>(My, B) && hxp % B == 0 && ypipe_smem<T>(My, B) <= budget)
-                CUDA_TRY(cudaFuncSetAttribute(ypipe_kernel<T>(My, B), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)ypipe_smem<T>(My, B)));
+                TRY(raise_smem_cap((const void*)ypipe_kernel<T>(My, B), ypipe_smem<T>(My, B)));
             if (fast_z && zpipe_kernel<T>(Mz, B) && hxp % B == 0 && zpipe_smem<T>(Mz, B) <= budget)
-                CUDA_TRY(cudaFuncSetAttribute(zpipe_kernel<T>(Mz, B), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                              (int)zpipe_smem<T>(Mz, B)));
+                TRY(raise_smem_cap((const void*)zpipe_kernel<T>(Mz, B), zpipe_smem<T>(Mz, B)));
         }
-        CUDA_TRY(cudaFuncSetAttribute(k_fft_x_r2c<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
-        CUDA_TRY(cudaFuncSetAttribute(k_fft_x_c2r<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_x));
-        CUDA_TRY(cudaFuncSetAttribute(k_fft_y<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_y));
-        CUDA_TRY(cudaFuncSetAttribute(k_fft_z_stokes<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_z));
+        TRY(raise_smem_cap((const void*)k_fft_x_r2c<T>, smem_x));
+        TRY(raise_smem_cap((const void*)k_fft_x_c2r<T>, smem_x));
+        TRY(raise_smem_cap((const void*)k_fft_y<T>, smem_y));
+        TRY(raise_smem_cap((const void*)k_fft_z_stokes<T>, smem_z));
         if (smem_stencil > 48 * 1024) {
-            CUDA_TRY(cudaFuncSetAttribute(k_spread_atomic<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_stencil));
-            CUDA_TRY(cudaFuncSetAttribute(k_interpolate_warp<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_stencil));
+            TRY(raise_smem_cap((const void*)k_spread_atomic<T>, smem_stencil));
+            TRY(raise_smem_cap((const void*)k_interpolate_warp<T>, smem_stencil));
+            TRY(raise_smem_cap((const void*)k_adjoint_gather<T>, smem_stencil));
         }
 
         // buffers
@@ -690,10 +725,10 @@ struct Engine final : EngineBase {
     // spectrum, y/z passes, then x-c2r fused with the interpolation.
     bool fused_available() const { return slab; }
 
-    int spread_to_spectrum(cudaStream_t s) {
+    int spread_to_spectrum(cudaStream_t s, const vec4<T>* force = nullptr) {
         StageScope sc(h, FFCM_STAGE_SPREAD, s);
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys, (const vec4<T>*)Fs,
+        return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys, force ? force : (const vec4<T>*)Fs,
                       (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, slab_lists,
                       slab_counts);
     }
@@ -721,7 +756,11 @@ struct Engine final : EngineBase {
                       (const int*)slab_lists, (const int*)slab_counts);
     }
 
-    int mobility_rest(void* V, cudaStream_t s) override {
+    int mobility_rest(void* V, cudaStream_t s) override { return solve(V, s, false); }
+
+    // keep_u: also leave the velocity grid u = L^-1 S F in gu (the adjoint's
+    // only checkpoint); the unfused pipeline leaves it there anyway.
+    int solve(void* V, cudaStream_t s, bool keep_u) {
         if (!slab) {
             TRY(spread(s));
             TRY(stokes(s));
@@ -730,6 +769,10 @@ struct Engine final : EngineBase {
         }
         TRY(spread_to_spectrum(s));
         TRY(stokes_yz(s));
+        if (keep_u) {
+            StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
+            TRY(x_inverse(gu, s));
+        }
         TRY(interp_from_spectrum(s));
         StageScope sc(h, FFCM_STAGE_CORRECT, s);
         return launch(h, k_correct<T>, grid_for(N, 128), 128, 0, s, N, (const vec4<T>*)Ys,
@@ -737,14 +780,83 @@ struct Engine final : EngineBase {
                       static_cast<T*>(V), cc, (const T*)partial, h3);
     }
 
-    int spread(cudaStream_t s) override {
-        // step API (spread_forces!): depends on Y_sorted/F_sorted only, as the
-        // reference's, so it does not use the cell-list-driven slab kernel
+    int spread(cudaStream_t s) override { return spread_from((const vec4<T>*)Fs, s); }
+
+    // step API (spread_forces!): depends on Y_sorted/F_sorted only, as the
+    // reference's, so it does not use the cell-list-driven slab kernel
+    int spread_from(const vec4<T>* force, cudaStream_t s) {
         TRY(ensure_real_grids());
         StageScope sc(h, FFCM_STAGE_SPREAD, s);
         CUDA_TRY(cudaMemsetAsync(gf, 0, 3 * (size_t)plane * sizeof(T), s));
         return launch(h, k_spread_atomic<T>, grid_for((int64_t)N * 32, 256, 148 * 64), 256,
-                      smem_stencil, s, N, (const vec4<T>*)Ys, (const vec4<T>*)Fs, gf, sp);
+                      smem_stencil, s, N, (const vec4<T>*)Ys, force, gf, sp);
+    }
+
+    int forward_checkpoint(void* V, cudaStream_t s) override {
+        TRY(ensure_adjoint());
+        return solve(V, s, true);
+    }
+
+    int ensure_adjoint() override {
+        TRY(ensure_real_grids());
+        if (gpsi) return FFCM_OK;
+        TRY(alloc(Ls, N));
+        TRY(alloc(Lin, 3 * (size_t)N));
+        TRY(alloc(dYo, 3 * (size_t)N));
+        TRY(alloc(dFo, 3 * (size_t)N));
+        TRY(alloc(Vt, 3 * (size_t)N));
+        TRY(alloc(Jd, 1));
+        TRY(alloc(gpsi, 3 * (size_t)plane));
+        CUDA_TRY(cudaMemset(Ls, 0, (size_t)N * sizeof(vec4<T>)));
+        CUDA_TRY(cudaMemset(gpsi, 0, 3 * (size_t)plane * sizeof(T)));
+        return FFCM_OK;
+    }
+
+    void* adj_buf(int which) override {
+        switch (which) {
+            case 0: return Lin;
+            case 1: return dYo;
+            case 2: return dFo;
+            case 3: return Vt;
+            default: return Jd;
+        }
+    }
+
+    // Pullback at cotangent lam of the last checkpointed forward (cell list,
+    // sorted Y/F and the velocity grid u still in place): psi = L^-1 S lam,
+    // then one stencil gather over (u, psi) and one pair pass.
+    int adjoint(const void* lam, void* dY, void* dF, cudaStream_t s) override {
+        TRY(ensure_adjoint());
+        {
+            StageScope sc(h, FFCM_STAGE_CELL_LIST, s);
+            TRY(launch(h, k_gather_forces<T>, grid_for(N, 256), 256, 0, s, N, (const int32_t*)perm,
+                       static_cast<const T*>(lam), Ls));
+        }
+        if (slab) {
+            TRY(spread_to_spectrum(s, Ls));
+            TRY(stokes_yz(s));
+            StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
+            TRY(x_inverse(gpsi, s));
+        } else {
+            TRY(spread_from(Ls, s));
+            TRY(stokes_to(gpsi, s));
+        }
+        {
+            StageScope sc(h, FFCM_STAGE_INTERPOLATE, s);
+            TRY(launch(h, k_adjoint_gather<T>, grid_for((int64_t)N * 32, 256, 148 * 64), 256, smem_stencil, s, N,
+                       (const vec4<T>*)Ys, (const vec4<T>*)Fs, (const vec4<T>*)Ls, (const int32_t*)perm,
+                       (const T*)gu, (const T*)gpsi, static_cast<T*>(dY), static_cast<T*>(dF), sp, h3));
+        }
+        StageScope sc(h, FFCM_STAGE_CORRECT, s);
+        return launch(h, k_correct_adjoint<T>, grid_for(N, 128), 128, 0, s, N, (const vec4<T>*)Ys,
+                      (const vec4<T>*)Fs, (const vec4<T>*)Ls, (const int32_t*)off, (const int32_t*)perm,
+                      static_cast<T*>(dY), static_cast<T*>(dF), cc, cgc);
+    }
+
+    int residual(const void* V, const void* Vtg, void* lam, double* J, cudaStream_t s) override {
+        CUDA_TRY(cudaMemsetAsync(J, 0, sizeof(double), s));
+        return launch(h, k_residual<T>, grid_for(3 * (int64_t)N, 256, 148 * 8), 256, 0, s, 3 * N,
+                      static_cast<const T*>(V), static_cast<const T*>(Vtg), static_cast<T*>(lam), J);
     }
 
     int launch_y(cudaStream_t s, int inverse) {
@@ -781,17 +893,36 @@ struct Engine final : EngineBase {
 
     int stokes(cudaStream_t s) override {
         TRY(ensure_real_grids());
+        return stokes_to(gu, s);
+    }
+
+    int x_forward(const T* in, cudaStream_t s) {
         const int nrows = 3 * My * Mz;
+        if (fast_x) {
+            const int H = Mx / 2;
+            return launch(h, xf_kernel<T>(H), (nrows + lpb_fx - 1) / lpb_fx, lpb_fx * (H / 8), smem_fx, s, in,
+                          spec, nrows, hxp, (const cplx<T>*)twx, lpb_fx);
+        }
+        return launch(h, k_fft_x_r2c<T>, (nrows + lpb_x - 1) / lpb_x, 256, smem_x, s, in, spec, Mx, nrows, hxp,
+                      plan_x, (const cplx<T>*)twx, lpb_x);
+    }
+
+    int x_inverse(T* out, cudaStream_t s) {
+        const int nrows = 3 * My * Mz;
+        if (fast_x) {
+            const int H = Mx / 2;
+            return launch(h, xi_kernel<T>(H), (nrows + lpb_fx - 1) / lpb_fx, lpb_fx * (H / 8), smem_fx, s,
+                          (const cplx<T>*)spec, out, nrows, hxp, (const cplx<T>*)twx, lpb_fx);
+        }
+        return launch(h, k_fft_x_c2r<T>, (nrows + lpb_x - 1) / lpb_x, 256, smem_x, s, (const cplx<T>*)spec, out,
+                      Mx, nrows, hxp, plan_x, (const cplx<T>*)twx, lpb_x);
+    }
+
+    // gf -> out through the full transform and the Stokes projector.
+    int stokes_to(T* out, cudaStream_t s) {
         {
             StageScope sc(h, FFCM_STAGE_FFT_X_FWD, s);
-            if (fast_x) {
-                const int H = Mx / 2;
-                TRY(launch(h, xf_kernel<T>(H), (nrows + lpb_fx - 1) / lpb_fx, lpb_fx * (H / 8), smem_fx, s,
-                           (const T*)gf, spec, nrows, hxp, (const cplx<T>*)twx, lpb_fx));
-            } else {
-                TRY(launch(h, k_fft_x_r2c<T>, (nrows + lpb_x - 1) / lpb_x, 256, smem_x, s,
-                           (const T*)gf, spec, Mx, nrows, hxp, plan_x, (const cplx<T>*)twx, lpb_x));
-            }
+            TRY(x_forward(gf, s));
         }
         {
             StageScope sc(h, FFCM_STAGE_FFT_Y_FWD, s);
@@ -806,13 +937,7 @@ struct Engine final : EngineBase {
             TRY(launch_y(s, 1));
         }
         StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
-        if (fast_x) {
-            const int H = Mx / 2;
-            return launch(h, xi_kernel<T>(H), (nrows + lpb_fx - 1) / lpb_fx, lpb_fx * (H / 8), smem_fx, s,
-                          (const cplx<T>*)spec, gu, nrows, hxp, (const cplx<T>*)twx, lpb_fx);
-        }
-        return launch(h, k_fft_x_c2r<T>, (nrows + lpb_x - 1) / lpb_x, 256, smem_x, s,
-                      (const cplx<T>*)spec, gu, Mx, nrows, hxp, plan_x, (const cplx<T>*)twx, lpb_x);
+        return x_inverse(out, s);
     }
 
     int interp(void* V, cudaStream_t s) override {
@@ -1003,6 +1128,7 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
                   void* stream) {
     g_err.clear();
     TRY(check_handle(h));
+    h->ckpt = false;
     TRY(check_memory(memory));
     const int64_t N = h->N;
     if (!(vr == 3 && vc == N && yr == 3 && yc == N && fr == 3 && fc == N)) {
@@ -1044,6 +1170,7 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
 int ffcm_wrap_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
+    h->ckpt = false;
     TRY(check_memory(memory));
     if (!Y) return fail(FFCM_ERR_ARGUMENT, "Y must not be NULL");
     DeviceGuard g(h->device);
@@ -1061,6 +1188,7 @@ int ffcm_wrap_positions(ffcm_handle* h, const void* Y, int32_t memory, void* str
 int ffcm_assign_cells(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
+    h->ckpt = false;
     DeviceGuard g(h->device);
     return h->eng->wrap_hash(nullptr, false, true, h->pick(stream));
 }
@@ -1068,6 +1196,7 @@ int ffcm_assign_cells(ffcm_handle* h, void* stream) {
 int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
+    h->ckpt = false;
     TRY(check_memory(memory));
     if (!F) return fail(FFCM_ERR_ARGUMENT, "F must not be NULL");
     DeviceGuard g(h->device);
@@ -1085,6 +1214,7 @@ int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, v
 int ffcm_spread_forces(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
+    h->ckpt = false;
     DeviceGuard g(h->device);
     return h->eng->spread(h->pick(stream));
 }
@@ -1092,6 +1222,7 @@ int ffcm_spread_forces(ffcm_handle* h, void* stream) {
 int ffcm_stokes_solve(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
+    h->ckpt = false;
     DeviceGuard g(h->device);
     return h->eng->stokes(h->pick(stream));
 }
@@ -1123,6 +1254,122 @@ int ffcm_correct_velocities(ffcm_handle* h, void* V, int32_t memory, void* strea
     TRY(h->eng->correct(h->eng->V_out(), s));
     CUDA_TRY(cudaMemcpyAsync(V, h->eng->V_out(), bytes, cudaMemcpyDeviceToHost, s));
     return finish(h, s);
+}
+
+int ffcm_mobility_checkpoint(ffcm_handle* h, void* V, const void* Y, const void* F, int32_t memory,
+                             void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    TRY(check_memory(memory));
+    h->ckpt = false;
+    if (!V || !Y || !F) return fail(FFCM_ERR_ARGUMENT, "V, Y and F must not be NULL");
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    TRY(e->ensure_adjoint());
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    const void* Yd = Y;
+    const void* Fd = F;
+    void* Vd = V;
+    if (memory == FFCM_HOST) {
+        StageScope sc(h, FFCM_STAGE_H2D, s);
+        CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(e->F_in(), F, bytes, cudaMemcpyHostToDevice, s));
+        Yd = e->Y_in();
+        Fd = e->F_in();
+        Vd = e->V_out();
+    }
+    TRY(e->wrap_hash(Yd, true, true, s));
+    TRY(e->sort(Fd, s));
+    TRY(e->forward_checkpoint(Vd, s));
+    h->ckpt = true;
+    if (memory == FFCM_HOST) {
+        {
+            StageScope sc(h, FFCM_STAGE_D2H, s);
+            CUDA_TRY(cudaMemcpyAsync(V, e->V_out(), bytes, cudaMemcpyDeviceToHost, s));
+        }
+        const int rc = finish(h, s);
+        if (rc != FFCM_OK) h->ckpt = false;
+        return rc;
+    }
+    return FFCM_OK;
+}
+
+int ffcm_adjoint(ffcm_handle* h, void* dJdY, void* dJdF, const void* lambda, int32_t memory, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    TRY(check_memory(memory));
+    if (!dJdY || !dJdF || !lambda) return fail(FFCM_ERR_ARGUMENT, "dJdY, dJdF and lambda must not be NULL");
+    if (!h->ckpt)
+        return fail(FFCM_ERR_STATE,
+                    "ffcm_adjoint needs the state of a preceding ffcm_mobility_checkpoint on this handle, "
+                    "with no other solve or step call in between");
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    if (memory == FFCM_DEVICE) return e->adjoint(lambda, dJdY, dJdF, s);
+    {
+        StageScope sc(h, FFCM_STAGE_H2D, s);
+        CUDA_TRY(cudaMemcpyAsync(e->adj_buf(0), lambda, bytes, cudaMemcpyHostToDevice, s));
+    }
+    TRY(e->adjoint(e->adj_buf(0), e->adj_buf(1), e->adj_buf(2), s));
+    {
+        StageScope sc(h, FFCM_STAGE_D2H, s);
+        CUDA_TRY(cudaMemcpyAsync(dJdY, e->adj_buf(1), bytes, cudaMemcpyDeviceToHost, s));
+        CUDA_TRY(cudaMemcpyAsync(dJdF, e->adj_buf(2), bytes, cudaMemcpyDeviceToHost, s));
+    }
+    return finish(h, s);
+}
+
+int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, void* V, const void* Y,
+                            const void* F, const void* V_target, int32_t memory, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    TRY(check_memory(memory));
+    h->ckpt = false;
+    if (!J || !dJdY || !dJdF || !V || !Y || !F || !V_target)
+        return fail(FFCM_ERR_ARGUMENT, "no argument of ffcm_objective_gradient may be NULL");
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    TRY(e->ensure_adjoint());
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    const void *Yd = Y, *Fd = F, *Td = V_target;
+    void *Vd = V, *dYd = dJdY, *dFd = dJdF;
+    double* Jdev = static_cast<double*>(e->adj_buf(4));
+    if (memory == FFCM_HOST) {
+        StageScope sc(h, FFCM_STAGE_H2D, s);
+        CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(e->F_in(), F, bytes, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(e->adj_buf(3), V_target, bytes, cudaMemcpyHostToDevice, s));
+        Yd = e->Y_in();
+        Fd = e->F_in();
+        Td = e->adj_buf(3);
+        Vd = e->V_out();
+        dYd = e->adj_buf(1);
+        dFd = e->adj_buf(2);
+    }
+    TRY(e->wrap_hash(Yd, true, true, s));
+    TRY(e->sort(Fd, s));
+    TRY(e->forward_checkpoint(Vd, s));
+    TRY(e->residual(Vd, Td, e->adj_buf(0), Jdev, s));
+    TRY(e->adjoint(e->adj_buf(0), dYd, dFd, s));
+    h->ckpt = true;
+    if (memory == FFCM_HOST) {
+        {
+            StageScope sc(h, FFCM_STAGE_D2H, s);
+            CUDA_TRY(cudaMemcpyAsync(V, Vd, bytes, cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaMemcpyAsync(dJdY, dYd, bytes, cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaMemcpyAsync(dJdF, dFd, bytes, cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaMemcpyAsync(J, Jdev, sizeof(double), cudaMemcpyDeviceToHost, s));
+        }
+        const int rc = finish(h, s);
+        if (rc != FFCM_OK) h->ckpt = false;
+        return rc;
+    }
+    CUDA_TRY(cudaMemcpyAsync(J, Jdev, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return FFCM_OK;
 }
 
 int64_t ffcm_buffer_bytes(const ffcm_handle* h, int32_t which) {
@@ -1266,6 +1513,7 @@ int ffcm_set_buffer(ffcm_handle* h, int32_t which, const void* src, int64_t nbyt
 int ffcm_synchronize(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
+    h->ckpt = false;
     DeviceGuard g(h->device);
     return finish(h, h->pick(stream));
 }

@@ -211,6 +211,30 @@ int ffcm_batch_mobility(ffcm_batch* b, void* V, const void* Y, const void* F, in
 int ffcm_batch_get_info(const ffcm_batch* b, int64_t* total_particles, int64_t* nsys,
                         int32_t* nrhs, int64_t* kernels_per_call);
 
+/* ---- adjoint form ---------------------------------------------------------
+ * Reverse-mode derivative of V = M(Y) F. No reference counterpart: the
+ * reference has no derivative; these are the two halves of a
+ * ChainRulesCore.rrule for mobility (src/mobility.jl:309-331), the forward
+ * half keeping only the velocity grid u = L^-1 S F (plus the cell list and
+ * sorted particles it already holds) and the pullback recomputing stencil
+ * weights. All arrays are 3xN in the handle's type. */
+
+/* Forward solve exactly as ffcm_mobility, which also keeps the checkpoint. */
+int ffcm_mobility_checkpoint(ffcm_handle* h, void* V, const void* Y, const void* F, int32_t memory,
+                             void* stream);
+/* Pullback at the cotangent lambda = dJ/dV of the last ffcm_mobility_checkpoint
+ * on this handle: dJdF = M lambda (M is symmetric) and
+ * dJdY_n = h^3 sum_g grad w_n(g) [lambda_n . u_g + F_n . psi_g]
+ *        + sum_m grad_x [lambda_n . T(x) F_m + lambda_m . T(x) F_n],
+ * psi = L^-1 S lambda, T the pair correction. FFCM_ERR_STATE if any other
+ * solve or step call ran on the handle since the checkpoint. */
+int ffcm_adjoint(ffcm_handle* h, void* dJdY, void* dJdF, const void* lambda, int32_t memory, void* stream);
+/* J = 0.5 |M(Y) F - V_target|^2 with dJ/dY, dJ/dF and V in one call
+ * (checkpointed forward, residual, pullback). J is a double in the same
+ * memory space as the arrays. */
+int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, void* V, const void* Y,
+                            const void* F, const void* V_target, int32_t memory, void* stream);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* Start recording CUDA events around every stage of every call. */

@@ -393,6 +393,71 @@ def apply(cfg, Y, F):
 
 
 # ----------------------------------------------------------------------------
+# Adjoint (vector-Jacobian product) of the mobility product. The reference
+# ships no derivative; this differentiates the restatement above and is pinned
+# in the tests by central finite differences of `mobility` in Float64.
+# ----------------------------------------------------------------------------
+
+def correction_scalars_d(r, sigma, Sigma, mu):
+    """(A, B, dA/dr, dB/dr) of src/correct_velocities.jl:71-104."""
+    T = np.asarray(sigma).dtype.type
+    ct = _ct(T)
+    A, B, dA, dB = ct(), ct(), ct(), ct()
+    getattr(lib(), "oracle_correction_scalars_d" + _sfx(T))(
+        ct(r), ct(sigma), ct(Sigma), ct(mu), ctypes.byref(A), ctypes.byref(B), ctypes.byref(dA),
+        ctypes.byref(dB))
+    return T(A.value), T(B.value), T(dA.value), T(dB.value)
+
+
+def adjoint(cfg, Y, F, lam):
+    """Pullback of V = M(Y) F at cotangent `lam` -> (V, dY, dF).
+
+    dF = M lam (M is symmetric); dY is the grid term h^3 sum_g grad w [lam.u + F.psi]
+    (u = L^-1 S F kept from the forward, psi = L^-1 S lam) plus the pair term.
+    """
+    T = cfg.T
+    N = cfg.N
+    Y = _as_particles(Y, T, N)
+    F = _as_particles(F, T, N)
+    lam = _as_particles(lam, T, N)
+    ct = _ct(T)
+    V = np.zeros((N, 3), T)
+    mobility(V, cfg, Y, F)
+    u = cfg.fluid_velocity.copy()
+    F_sorted = cfg.F_sorted.copy()
+    L_sorted = np.ascontiguousarray(lam[cfg.original_index.astype(np.int64) - 1])
+    cfg.F_sorted[...] = L_sorted
+    spread_forces(cfg)
+    stokes_solve(cfg)
+    psi = cfg.fluid_velocity
+    dF = np.zeros((N, 3), T)
+    interpolate_velocities(dF, cfg)
+    correct_velocities(dF, cfg)
+    cfg.F_sorted[...] = F_sorted
+    dY = np.zeros((N, 3), T)
+    getattr(lib(), "oracle_grad_gather" + _sfx(T))(
+        _p(dY), _p(u), _p(psi), _p(cfg.Y_sorted), _p(F_sorted), _p(L_sorted),
+        _p(cfg.original_index), ctypes.c_int64(N), ct(cfg.sigma), ct(cfg.Sigma), ct(cfg.h),
+        ct(cfg.inv_h), _p(cfg.M_arr), ctypes.c_int32(cfg.M_G))
+    getattr(lib(), "oracle_correct_grad" + _sfx(T))(
+        _p(dY), _p(cfg.Y_sorted), _p(F_sorted), _p(L_sorted), _p(cfg.cell_start),
+        _p(cfg.cell_end), _p(cfg.original_index), _p(cfg.num_cells_arr), _p(cfg.L_arr),
+        ct(cfg.sigma), ct(cfg.Sigma), ct(cfg.mu), ct(cfg.R_c))
+    cfg.fluid_velocity[...] = u
+    return V, dY, dF
+
+
+def objective_gradient(cfg, Y, F, V_target):
+    """J = 0.5 |M(Y) F - V_target|^2 and its gradients -> (J, dJ/dY, dJ/dF, V)."""
+    T = cfg.T
+    V = apply(cfg, Y, F)
+    lam = (V - np.asarray(V_target, T)).astype(T)
+    V, dY, dF = adjoint(cfg, Y, F, lam)
+    J = 0.5 * float(np.sum(lam.astype(np.float64) ** 2))
+    return J, dY, dF, V
+
+
+# ----------------------------------------------------------------------------
 # Closed-form references used by the reference's own tests
 # ----------------------------------------------------------------------------
 

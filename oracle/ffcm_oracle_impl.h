@@ -308,6 +308,163 @@ void FN(oracle_correct)(FT* V, const FT* Y_sorted, const FT* F_sorted, const int
     }
 }
 
+/* ---------------------------------------------------------------------------
+ * Adjoint of the mobility product (the reference has no derivative code; this
+ * differentiates the forward restatement above, and the test suite pins it
+ * with central finite differences of that forward in Float64).
+ *
+ * For the cotangent lam of V = M(Y) F:
+ *   dY_n = h^3 sum_g grad_Y w_n(g) [lam_n . u_g + F_n . psi_g]
+ *        + sum_m grad_x [lam_n . T(x) F_m + lam_m . T(x) F_n],  x = Y_n - Y_m
+ * with u = L^-1 S F, psi = L^-1 S lam and T(x) = A(r) I + B(r) x x^T.
+ * ------------------------------------------------------------------------- */
+
+/* r-derivatives of the pair scalars of src/correct_velocities.jl:71-104,
+ * term by term from the expression above (product and chain rules). */
+void FN(oracle_correction_scalars_d)(FT r, FT sigma, FT Sigma, FT mu, FT* A, FT* B, FT* dA,
+                                     FT* dB) {
+    FN(oracle_correction_scalars)(r, sigma, Sigma, mu, A, B);
+    FT r2 = r * r, r3 = r2 * r, r4 = r2 * r2, r5 = r4 * r, r6 = r3 * r3;
+    FT s2 = sigma * sigma, s4 = s2 * s2, S2 = Sigma * Sigma, S4 = S2 * S2;
+    FT d = s2 - S2;
+    FT dq = d * d / (FT)4;
+    FT pi = (FT)PI_T;
+    FT fourpimu = (FT)4 * pi * mu;
+    FT eightpimu = (FT)8 * pi * mu;
+    FT erf_diff = (FT)ERF(r / ((FT)2 * sigma)) - (FT)ERF(r / ((FT)2 * Sigma));
+    FT es = (FT)EXP(-r2 / ((FT)4 * s2)), eS = (FT)EXP(-r2 / ((FT)4 * S2));
+    /* d/dr erf(r / (2w)) = exp(-r^2 / (4 w^2)) / (w sqrt(pi)) */
+    FT derf = es / (sigma * (FT)SQRT(pi)) - eS / (Sigma * (FT)SQRT(pi));
+    FT Ds = (FT)POW((FT)4 * pi * s2, -(FT)3 / (FT)2) * es;
+    FT DS = (FT)POW((FT)4 * pi * S2, -(FT)3 / (FT)2) * eS;
+    FT dDs = -r / ((FT)2 * s2) * Ds, dDS = -r / ((FT)2 * S2) * DS;
+    FT PA = (FT)2 * S4 / (mu * r2) + d / mu * ((FT)1 + (FT)2 * S2 / r2) -
+            dq * ((FT)2 - r2 / ((FT)2 * S2)) / ((FT)2 * mu * S2);
+    FT dPA = -(FT)4 * S4 / (mu * r3) - (FT)4 * d * S2 / (mu * r3) + dq * r / ((FT)2 * mu * S2 * S2);
+    FT PB = -(FT)6 * S4 / (mu * r4) - d / (mu * r2) * ((FT)1 + (FT)6 * S2 / r2) - dq / ((FT)4 * mu * S4);
+    FT dPB = (FT)24 * S4 / (mu * r5) + (FT)2 * d / (mu * r3) + (FT)24 * d * S2 / (mu * r5);
+    *dA = derf * ((FT)1 / (eightpimu * r) + s2 / (fourpimu * r3)) +
+          erf_diff * (-(FT)1 / (eightpimu * r2) - (FT)3 * s2 / (fourpimu * r4)) -
+          (FT)2 * s4 / mu * (dDs / r2 - (FT)2 * Ds / r3) + dPA * DS + PA * dDS;
+    *dB = derf * ((FT)1 / (eightpimu * r3) - (FT)3 * s2 / (fourpimu * r5)) +
+          erf_diff * (-(FT)3 / (eightpimu * r4) + (FT)15 * s2 / (fourpimu * r6)) +
+          (FT)6 * s4 / mu * (dDs / r4 - (FT)4 * Ds / r5) + dPB * DS + PB * dDS;
+}
+
+/* Grid part of dY (overwrite): one pass over each particle's stencil, with
+ * the weight gradient per axis  d w / d Y_i = w_g * x_i * [(a0 + a2 r^2)/Sigma^2 - 2 a2]
+ * where w_g = g_x g_y g_z and x = grid point - Y (stencil of src/stencil.jl:80-112). */
+void FN(oracle_grad_gather)(FT* dY, const FT* u, const FT* psi, const FT* Y_sorted,
+                            const FT* F_sorted, const FT* L_sorted, const int32_t* original_index,
+                            int64_t N, FT sigma, FT Sigma, FT h, FT inv_h, const int32_t* M,
+                            int32_t MG) {
+    int64_t Mtot = (int64_t)M[0] * M[1] * M[2];
+    FT c4[4];
+    FN(oracle_modified_kernel_coefficients)(sigma, Sigma, c4);
+    FT a0 = c4[0], a2 = c4[1], inv_norm = c4[2], inv_2S2 = c4[3];
+    FT inv_S2 = (FT)2 * inv_2S2;
+    FT h3 = h * h * h;
+    FT* g = (FT*)malloc(sizeof(FT) * 3 * MG);
+    FT* r2 = (FT*)malloc(sizeof(FT) * 3 * MG);
+    FT* xo = (FT*)malloc(sizeof(FT) * 3 * MG);
+    int32_t* idx = (int32_t*)malloc(sizeof(int32_t) * 3 * MG);
+    int32_t half = MG / 2;
+    for (int64_t s = 0; s < N; ++s) {
+        const FT* Yn = Y_sorted + 3 * s;
+        const FT* Fn = F_sorted + 3 * s;
+        const FT* Ln = L_sorted + 3 * s;
+        FN(fill_stencil)(g, r2, idx, Yn, inv_norm, inv_2S2, h, inv_h, M, MG);
+        for (int i = 0; i < 3; ++i) {
+            int32_t j = (int32_t)RINT(Yn[i] * inv_h);
+            for (int32_t k = 0; k < MG; ++k) xo[i * MG + k] = (FT)(j + k - half) * h - Yn[i];
+        }
+        FT d0 = 0, d1 = 0, d2 = 0;
+        for (int32_t kz = 0; kz < MG; ++kz)
+            for (int32_t ky = 0; ky < MG; ++ky)
+                for (int32_t kx = 0; kx < MG; ++kx) {
+                    int64_t o = (idx[2 * MG + kz] * (int64_t)M[1] + idx[MG + ky]) * M[0] + idx[kx];
+                    FT rr = r2[kx] + r2[MG + ky] + r2[2 * MG + kz];
+                    FT gg = g[kx] * g[MG + ky] * g[2 * MG + kz];
+                    FT fac = gg * ((a0 + a2 * rr) * inv_S2 - (FT)2 * a2);
+                    FT sg = Ln[0] * u[o] + Ln[1] * u[Mtot + o] + Ln[2] * u[2 * Mtot + o] +
+                            Fn[0] * psi[o] + Fn[1] * psi[Mtot + o] + Fn[2] * psi[2 * Mtot + o];
+                    FT c = fac * sg;
+                    d0 += c * xo[kx];
+                    d1 += c * xo[MG + ky];
+                    d2 += c * xo[2 * MG + kz];
+                }
+        int64_t n = (int64_t)original_index[s] - 1;
+        dY[3 * n] = h3 * d0;
+        dY[3 * n + 1] = h3 * d1;
+        dY[3 * n + 2] = h3 * d2;
+    }
+    free(g); free(r2); free(xo); free(idx);
+}
+
+/* Pair part of dY (accumulate): the neighbour loop of oracle_correct with
+ * grad_x [lam_n.T F_m + lam_m.T F_n]
+ *   = (A' P + B' Q) x / r + B [lam_n (x.F_m) + F_m (lam_n.x) + lam_m (x.F_n) + F_n (lam_m.x)],
+ * P = lam_n.F_m + lam_m.F_n, Q = (lam_n.x)(x.F_m) + (lam_m.x)(x.F_n). */
+void FN(oracle_correct_grad)(FT* dY, const FT* Y_sorted, const FT* F_sorted, const FT* L_sorted,
+                             const int32_t* cell_start, const int32_t* cell_end,
+                             const int32_t* original_index, const int32_t* num_cells, const FT* L,
+                             FT sigma, FT Sigma, FT mu, FT R_c) {
+    FT Rc2 = R_c * R_c;
+    int32_t mx = num_cells[0], my = num_cells[1], mz = num_cells[2];
+    for (int32_t cz = 0; cz < mz; ++cz)
+    for (int32_t cy = 0; cy < my; ++cy)
+    for (int32_t cx = 0; cx < mx; ++cx) {
+        int32_t c = cx + (cy + cz * my) * mx;
+        for (int32_t s = cell_start[c]; s <= cell_end[c]; ++s) {
+            const FT* Yn = Y_sorted + 3 * (int64_t)(s - 1);
+            const FT* Fn = F_sorted + 3 * (int64_t)(s - 1);
+            const FT* Ln = L_sorted + 3 * (int64_t)(s - 1);
+            FT gr[3] = {0, 0, 0};
+            for (int32_t dz = -1; dz <= 1; ++dz) {
+                int32_t nz = ((cz + dz) % mz + mz) % mz;
+                for (int32_t dy = -1; dy <= 1; ++dy) {
+                    int32_t ny = ((cy + dy) % my + my) % my;
+                    for (int32_t dx = -1; dx <= 1; ++dx) {
+                        int32_t nx = ((cx + dx) % mx + mx) % mx;
+                        int32_t cn = nx + (ny + nz * my) * mx;
+                        for (int32_t s2 = cell_start[cn]; s2 <= cell_end[cn]; ++s2) {
+                            if (s2 == s) continue;
+                            const FT* Ym = Y_sorted + 3 * (int64_t)(s2 - 1);
+                            FT x[3];
+                            for (int i = 0; i < 3; ++i) {
+                                FT t = Yn[i] - Ym[i];
+                                x[i] = t - L[i] * (FT)RINT(t / L[i]);
+                            }
+                            FT rr = x[0] * x[0] + x[1] * x[1] + x[2] * x[2];
+                            if (!(rr < Rc2)) continue;
+                            FT r = (FT)SQRT(rr);
+                            FT A, B, dA, dB;
+                            FN(oracle_correction_scalars_d)(r, sigma, Sigma, mu, &A, &B, &dA, &dB);
+                            const FT* Fm = F_sorted + 3 * (int64_t)(s2 - 1);
+                            const FT* Lm = L_sorted + 3 * (int64_t)(s2 - 1);
+                            FT P = Ln[0] * Fm[0] + Ln[1] * Fm[1] + Ln[2] * Fm[2] +
+                                   Lm[0] * Fn[0] + Lm[1] * Fn[1] + Lm[2] * Fn[2];
+                            FT lnx = Ln[0] * x[0] + Ln[1] * x[1] + Ln[2] * x[2];
+                            FT lmx = Lm[0] * x[0] + Lm[1] * x[1] + Lm[2] * x[2];
+                            FT xfm = x[0] * Fm[0] + x[1] * Fm[1] + x[2] * Fm[2];
+                            FT xfn = x[0] * Fn[0] + x[1] * Fn[1] + x[2] * Fn[2];
+                            FT Q = lnx * xfm + lmx * xfn;
+                            FT radial = (dA * P + dB * Q) / r;
+                            for (int i = 0; i < 3; ++i)
+                                gr[i] += radial * x[i] +
+                                         B * (Ln[i] * xfm + Fm[i] * lnx + Lm[i] * xfn + Fn[i] * lmx);
+                        }
+                    }
+                }
+            }
+            int64_t n = (int64_t)original_index[s - 1] - 1;
+            dY[3 * n] += gr[0];
+            dY[3 * n + 1] += gr[1];
+            dY[3 * n + 2] += gr[2];
+        }
+    }
+}
+
 #undef FN
 #undef CAT
 #undef CAT_

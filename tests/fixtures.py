@@ -63,8 +63,9 @@ def random_cloud(T, N, L, seed):
 
 
 def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None):
-    """Uniform i.i.d. positions in the cubic box [0, L)^3, rejection-sampled so
-    that no two centres are closer than `min_sep` (2a for unit spheres).
+    """Uniform i.i.d. positions in the box [0, L)^3 (L a scalar or a 3-tuple),
+    rejection-sampled so that no two centres are closer than `min_sep` (2a for
+    unit spheres).
 
     Candidates are drawn in batches; a candidate is kept when it is at least
     `min_sep` from every kept centre and from every other candidate of its batch
@@ -73,26 +74,33 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None):
     float64 positions of shape (N, 3) in random (shuffled) order.
     """
     rng = np.random.default_rng(seed)
-    L = float(L)
-    nc = max(int(np.floor(L / min_sep)), 3)
-    cs = L / nc
+    L = np.broadcast_to(np.asarray(L, np.float64), (3,)).copy()
+    phi = N * np.pi / 6.0 * min_sep ** 3 / float(np.prod(L))
+    if phi > 0.3:
+        raise ValueError(f"volume fraction {phi:.2f} is beyond what random sequential addition "
+                         "reaches in reasonable time (0.3)")
+    ncv = np.maximum(np.floor(L / min_sep).astype(np.int64), 3)
+    cs = L / ncv
     cap = 8
-    grid = -np.ones((nc, nc, nc, cap), np.int64)
-    fill = np.zeros((nc, nc, nc), np.int64)
+    grid = -np.ones((ncv[0], ncv[1], ncv[2], cap), np.int64)
+    fill = np.zeros((ncv[0], ncv[1], ncv[2]), np.int64)
     pos = np.empty((N, 3), np.float64)
     count = 0
     offs = np.array([(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)])
     ms2 = min_sep * min_sep
+    stalled = 0
     while count < N:
+        if stalled > 200:
+            raise RuntimeError(f"placed {count} of {N} spheres; no progress in 200 batches")
         need = N - count
         B = batch or max(1024, int(need * 1.3))
         cand = rng.random((B, 3)) * L
-        cc = np.minimum((cand / cs).astype(np.int64), nc - 1)
+        cc = np.minimum((cand / cs).astype(np.int64), ncv - 1)
         ok = np.ones(B, bool)
         # against kept centres
         cu = max(1, int(fill.max()))
         for o in offs:
-            nb = (cc + o) % nc
+            nb = (cc + o) % ncv
             occ = grid[nb[:, 0], nb[:, 1], nb[:, 2], :cu]     # (B, cu)
             valid = occ >= 0
             if not valid.any():
@@ -105,16 +113,16 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None):
         # within the batch: bucket candidates, compare against neighbours
         idx = np.nonzero(ok)[0]
         if idx.size:
-            key = (cc[idx, 0] * nc + cc[idx, 1]) * nc + cc[idx, 2]
+            key = (cc[idx, 0] * ncv[1] + cc[idx, 1]) * ncv[2] + cc[idx, 2]
             order = np.argsort(key, kind="stable")
             idx = idx[order]
             key = key[order]
             bad = np.zeros(B, bool)
-            starts = np.searchsorted(key, np.arange(nc ** 3))
-            ends = np.searchsorted(key, np.arange(nc ** 3), side="right")
+            starts = np.searchsorted(key, np.arange(int(np.prod(ncv))))
+            ends = np.searchsorted(key, np.arange(int(np.prod(ncv))), side="right")
             for o in offs:
-                nb = (cc[idx] + o) % nc
-                nk = (nb[:, 0] * nc + nb[:, 1]) * nc + nb[:, 2]
+                nb = (cc[idx] + o) % ncv
+                nk = (nb[:, 0] * ncv[1] + nb[:, 1]) * ncv[2] + nb[:, 2]
                 s0, s1 = starts[nk], ends[nk]
                 width = int((s1 - s0).max()) if idx.size else 0
                 for t in range(width):
@@ -132,7 +140,7 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None):
             ok &= ~bad
         acc = np.nonzero(ok)[0][:need]
         if acc.size:
-            flat = (cc[acc, 0] * nc + cc[acc, 1]) * nc + cc[acc, 2]
+            flat = (cc[acc, 0] * ncv[1] + cc[acc, 1]) * ncv[2] + cc[acc, 2]
             order = np.argsort(flat, kind="stable")
             acc, flat = acc[order], flat[order]
             first = np.searchsorted(flat, flat)             # first index of each cell group
@@ -144,6 +152,7 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None):
             np.maximum.at(fill.reshape(-1), flat, slot + 1)
             pos[count:count + acc.size] = cand[acc]
             count += acc.size
+        stalled = 0 if acc.size else stalled + 1
     perm = rng.permutation(N)
     return pos[perm]
 

@@ -277,3 +277,18 @@ def test_fused_and_unfused_paths_agree(ffcm, monkeypatch):
     Vc = _run(ffcm, fused, z["f32_Y"], z["f32_F"])
     Vd = _run(ffcm, fused, z["f32_Y"], z["f32_F"])
     assert rel_l2(Vc, Vd) < 1e-6
+
+
+def test_configurations_of_different_sizes_alive_at_once(ffcm):
+    """Kernel launch limits are per process, not per configuration: a smaller
+    configuration created later must not break an earlier, larger one."""
+    rng = np.random.default_rng(21)
+    big = ffcm.FFCMConfig(np.float64, **kw_of(27.0, 400, 48, R_c=3.0))
+    small = ffcm.FFCMConfig(np.float64, **kw_of(13.5, 50, 24, R_c=3.0))
+    for cfg, L in ((big, 27.0), (small, 13.5), (big, 27.0)):
+        Y = rng.random((cfg.N, 3)) * L
+        F = rng.standard_normal((cfg.N, 3))
+        V = np.empty_like(Y)
+        ffcm.mobility(V, cfg, Y, F)
+        ora = O.OracleConfig(np.float64, **kw_of(L, cfg.N, cfg.num_grid_points[0], R_c=3.0))
+        assert rel_l2(V, O.apply(ora, Y, F)) < 1e-10
