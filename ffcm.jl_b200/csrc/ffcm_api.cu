@@ -1750,3 +1750,171 @@ int ffcm_batch_mobility(ffcm_batch* b, void* V, const void* Y, const void* F, in
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Cell-list sort with library-owned scratch (no allocation per call).
+//
+// ffcm_sort_cells_noalloc computes the reference's three cell-list buffers
+// (original_index, cell_start, cell_end of src/cell_list.jl:64-93) from a
+// caller's cell_hash array, using only memory the caller passes in plus a
+// fixed scratch array that lives in this library's own device image. It never
+// calls cudaMalloc or cudaFree, nor anything that allocates on its behalf.
+//
+// Who needs this: an ffcm_handle allocates all of its buffers when it is
+// created, and holds them, which is right for repeated solves of one system.
+// A caller that builds cell lists for many differently sized systems, or that
+// runs under a fixed device-memory budget (a Julia or Python host that has
+// handed its memory to its own pool allocator, or an application that keeps
+// other streams busy and cannot afford the device-wide synchronisation that
+// cudaFree, and sometimes cudaMalloc, performs) cannot create a handle per
+// system. It can call this function with its own arrays instead.
+//
+// Limits and rules:
+//   * at most FFCM_NOALLOC_MAX_CELLS cells (the scratch holds two int32 arrays
+//     of that length plus the scan's tile sums, 16 MiB in total);
+//   * the scratch is one array per device: calls that overlap in time on one
+//     device (different streams, different host threads) race on it and must
+//     be serialised by the caller;
+//   * the first call on each device looks the scratch up with
+//     cudaGetSymbolAddress (which may load this library's device code onto
+//     that device); make that first call before any stream capture begins;
+//   * nothing needs to be zero beforehand: every call clears the counters it
+//     uses and its range-check flag before counting;
+//   * the call runs on the calling thread's current device, on `stream`, and
+//     returns after the sort is complete (it reads back the range-check flag).
+// ---------------------------------------------------------------------------
+
+namespace {
+
+constexpr int64_t kNoallocMaxCells = FFCM_NOALLOC_MAX_CELLS;
+constexpr int64_t kNoallocMaxTiles = (kNoallocMaxCells + SCAN_TILE - 1) / SCAN_TILE;
+// [0, C): per-cell counts, then per-cell cursors; [C, 2C+1): 0-based cell
+// offsets; then the scan's tile sums; the last word is the range-check flag.
+constexpr int64_t kNoallocScratchInts = 2 * kNoallocMaxCells + 1 + kNoallocMaxTiles + 1;
+
+}  // namespace
+
+static __device__ __align__(256) int32_t g_noalloc_scratch[kNoallocScratchInts];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+int32_t* g_noalloc_ptr[64] = {};
+
+// Resolve (once per device) the device address of the scratch array.
+int noalloc_scratch(int32_t** out) {
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return fail(FFCM_ERR_UNSUPPORTED, "device ordinal above 63");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(cell-sort scratch)");
+        g_noalloc_ptr[dev] = static_cast<int32_t*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return FFCM_OK;
+}
+
+// Zero a[0, n) and, when flag is given, the range-check flag.
+__global__ void k_noalloc_zero(int32_t* __restrict__ a, int n, int32_t* __restrict__ flag) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = 0;
+    if (flag && blockIdx.x == 0 && threadIdx.x == 0) *flag = 0;
+}
+
+// Histogram of the keys; a key outside [0, ncell) raises the flag and is skipped.
+__global__ void k_noalloc_count(int n_part, const int32_t* __restrict__ key, int ncell,
+                                int32_t* __restrict__ count, int32_t* __restrict__ flag) {
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_part; n += gridDim.x * blockDim.x) {
+        const int c = key[n];
+        if (c < 0 || c >= ncell) {
+            atomicOr(flag, 1);
+            continue;
+        }
+        atomicAdd(&count[c], 1);
+    }
+}
+
+__global__ void k_noalloc_scatter(int n_part, const int32_t* __restrict__ key, int ncell,
+                                  const int32_t* __restrict__ off, int32_t* __restrict__ cursor,
+                                  int32_t* __restrict__ slot_of) {
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < n_part; n += gridDim.x * blockDim.x) {
+        const int c = key[n];
+        if (c < 0 || c >= ncell) continue;
+        slot_of[off[c] + atomicAdd(&cursor[c], 1)] = n;
+    }
+}
+
+// Per cell: ascending original order (stability), 1-based indices, and the
+// reference's 1-based inclusive ranges (an empty cell has start = end + 1).
+__global__ void k_noalloc_finish(int ncell, const int32_t* __restrict__ off, int32_t* __restrict__ idx,
+                                 int32_t* __restrict__ cell_start, int32_t* __restrict__ cell_end) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
+        const int b = off[c], e = off[c + 1];
+        for (int i = b + 1; i < e; ++i) {
+            const int v = idx[i];
+            int j = i - 1;
+            while (j >= b && idx[j] > v) {
+                idx[j + 1] = idx[j];
+                --j;
+            }
+            idx[j + 1] = v;
+        }
+        for (int i = b; i < e; ++i) idx[i] += 1;
+        cell_start[c] = b + 1;
+        cell_end[c] = e;
+    }
+}
+
+}  // namespace
+
+extern "C" int ffcm_sort_cells_noalloc(const int32_t* cell_hash, int64_t N, int32_t ncell, int32_t* original_index,
+                            int32_t* cell_start, int32_t* cell_end, void* stream) {
+    g_err.clear();
+    if (N < 0 || N > (int64_t)std::numeric_limits<int32_t>::max())
+        return fail(FFCM_ERR_ARGUMENT, "N must be in [0, 2^31 - 1]; got " + std::to_string(N));
+    if (ncell < 1 || ncell > kNoallocMaxCells)
+        return fail(FFCM_ERR_ARGUMENT, "ncell must be in [1, " + std::to_string(kNoallocMaxCells) +
+                                           "] (the fixed scratch size); got " + std::to_string(ncell));
+    if ((N > 0 && (!cell_hash || !original_index)) || !cell_start || !cell_end)
+        return fail(FFCM_ERR_ARGUMENT, "cell_hash, original_index, cell_start and cell_end must not be NULL");
+    int32_t* scratch = nullptr;
+    TRY(noalloc_scratch(&scratch));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int n = (int)N;
+    int32_t* cnt = scratch;
+    int32_t* off = scratch + kNoallocMaxCells;
+    int32_t* tiles = off + kNoallocMaxCells + 1;
+    int32_t* flag = tiles + kNoallocMaxTiles;
+    const int ntiles = (ncell + SCAN_TILE - 1) / SCAN_TILE;
+    auto chk = [](const char* what) -> int {
+        const cudaError_t e = cudaGetLastError();
+        return e == cudaSuccess ? FFCM_OK : cuda_fail(e, what);
+    };
+    k_noalloc_zero<<<grid_for(ncell, 256), 256, 0, s>>>(cnt, ncell, flag);
+    TRY(chk("k_noalloc_zero"));
+    if (n > 0) {
+        k_noalloc_count<<<grid_for(n, 256), 256, 0, s>>>(n, cell_hash, ncell, cnt, flag);
+        TRY(chk("k_noalloc_count"));
+    }
+    k_scan_tiles<<<ntiles, SCAN_THREADS, 0, s>>>(cnt, ncell, tiles);
+    TRY(chk("k_scan_tiles"));
+    k_scan_tile_sums<<<1, 1024, 0, s>>>(tiles, ntiles);
+    TRY(chk("k_scan_tile_sums"));
+    k_scan_apply<<<ntiles, SCAN_THREADS, 0, s>>>(cnt, ncell, tiles, off);
+    TRY(chk("k_scan_apply"));
+    k_noalloc_zero<<<grid_for(ncell, 256), 256, 0, s>>>(cnt, ncell, nullptr);  // cursors; keep the flag
+    TRY(chk("k_noalloc_zero"));
+    if (n > 0) {
+        k_noalloc_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, cell_hash, ncell, off, cnt, original_index);
+        TRY(chk("k_noalloc_scatter"));
+    }
+    k_noalloc_finish<<<grid_for(ncell, 256), 256, 0, s>>>(ncell, off, original_index, cell_start, cell_end);
+    TRY(chk("k_noalloc_finish"));
+    int32_t bad = 0;
+    CUDA_TRY(cudaMemcpyAsync(&bad, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (bad) return fail(FFCM_ERR_ARGUMENT, "a cell_hash value lies outside [0, ncell)");
+    return FFCM_OK;
+}

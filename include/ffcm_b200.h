@@ -235,6 +235,26 @@ int ffcm_adjoint(ffcm_handle* h, void* dJdY, void* dJdF, const void* lambda, int
 int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, void* V, const void* Y,
                             const void* F, const void* V_target, int32_t memory, void* stream);
 
+/* ---- cell-list sort without allocation -------------------------------------
+ * No counterpart in the reference. Computes the reference's cell-list buffers
+ * (original_index, 1-based; cell_start and cell_end, 1-based inclusive, an
+ * empty cell having start = end + 1; src/cell_list.jl:64-93) from a device
+ * array of 0-based cell hashes, with the same stable order as
+ * ffcm_sort_particles_by_cell. It allocates no memory: its scratch is a fixed
+ * array inside the library, so callers that must not allocate per call (a
+ * host language that owns the device memory pool, or a program that cannot
+ * afford the device-wide synchronisation of cudaFree) can still build cell
+ * lists for systems of any N. Limits: ncell <= FFCM_NOALLOC_MAX_CELLS; one
+ * scratch per device, so calls that overlap in time on one device race and
+ * must be serialised by the caller; the first call on a device sets the
+ * scratch up and should come before any stream capture. All pointers are
+ * device pointers on the calling thread's current device; the call returns
+ * when the sort is complete. A hash outside [0, ncell) gives
+ * FFCM_ERR_ARGUMENT. */
+#define FFCM_NOALLOC_MAX_CELLS (1 << 21)
+int ffcm_sort_cells_noalloc(const int32_t* cell_hash, int64_t N, int32_t ncell, int32_t* original_index,
+                            int32_t* cell_start, int32_t* cell_end, void* stream);
+
 /* ---- measurement --------------------------------------------------------- */
 
 /* Start recording CUDA events around every stage of every call. */
