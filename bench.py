@@ -166,7 +166,7 @@ def measured_peak_hbm():
 
 def ncu_traffic(stage):
     """Per-launch DRAM bytes of a stage's kernel from the committed ncu summary."""
-    p = ROOT / "profiles" / "ncu_traffic_c2.txt"
+    p = ROOT / "profiles" / "ncu_traffic_plain_N500k_512cubed.txt"
     if not p.exists():
         return None
     for line in p.read_text().splitlines():
