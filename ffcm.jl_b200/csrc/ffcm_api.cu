@@ -314,6 +314,8 @@ struct Engine final : EngineBase {
     // y/z pass variant: 0 = one tile per block (k_fftp_*), 1 = persistent
     // pipelined (k_fftq_*); grid size of the persistent variant
     int ykind = 0, zkind = 0, ygrid = 0, zgrid = 0;
+    // kx columns per chunk of the y/z/y passes (0: one pass over the spectrum)
+    int kx_chunk = 0;
     int num_sms = 148;
     size_t smem_fx = 0, smem_fy = 0, smem_fz = 0;
     // slab kernels: spread/interpolation fused with the x transforms
@@ -668,6 +670,21 @@ struct Engine final : EngineBase {
                 }
             zkind = bk; Bz = bB; zgrid = bg;
         }
+        if (fast_y && fast_z) {
+            // chunk widths that keep a chunk's spectrum within ~96 MB of L2
+            const double col_bytes = 3.0 * My * Mz * sizeof(cplx<T>);
+            float best = 1e30f;
+            int bc = 0;
+            for (int c : {0, 64, 32, 16, 8, 4}) {
+                if (c > 0 && (c % By != 0 || c % Bz != 0 || c >= nkx || c * col_bytes > 96e6)) continue;
+                kx_chunk = c;
+                float ms = 0;
+                TRY(time_launches([&] { return stokes_yz(h->stream); }, ms));
+                if (verbose) fprintf(stderr, "ffcm autotune: yz chunk=%d %.4f ms\n", c, ms / 3);
+                if (ms < best) { best = ms; bc = c; }
+            }
+            kx_chunk = bc;
+        }
         CUDA_TRY(cudaStreamSynchronize(h->stream));
         h->launches = 0;
         return FFCM_OK;
@@ -733,7 +750,21 @@ struct Engine final : EngineBase {
                       slab_counts);
     }
 
+    // y forward, z + projector, y inverse. With kx chunking (kx_chunk > 0) the
+    // three passes run chunk by chunk, so a chunk's intermediate spectrum
+    // (3 My Mz kx_chunk values) stays in L2 between the passes and only the
+    // first read and the last write of each value reach HBM.
     int stokes_yz(cudaStream_t s) {
+        if (kx_chunk > 0 && kx_chunk < nkx) {
+            StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
+            for (int k0 = 0; k0 < nkx; k0 += kx_chunk) {
+                const int k1 = std::min(nkx, k0 + kx_chunk);
+                TRY(launch_y(s, 0, k0, k1));
+                TRY(launch_z(s, k0, k1));
+                TRY(launch_y(s, 1, k0, k1));
+            }
+            return FFCM_OK;
+        }
         {
             StageScope sc(h, FFCM_STAGE_FFT_Y_FWD, s);
             TRY(launch_y(s, 0));
@@ -859,31 +890,36 @@ struct Engine final : EngineBase {
                       static_cast<const T*>(V), static_cast<const T*>(Vtg), static_cast<T*>(lam), J);
     }
 
-    int launch_y(cudaStream_t s, int inverse) {
+    // y pass over the kx columns [k0, k1) (the whole spectrum when k1 <= 0).
+    int launch_y(cudaStream_t s, int inverse, int k0 = 0, int k1 = 0) {
+        if (k1 <= 0) k1 = nkx;
         if (fast_y && ykind == 1) {
-            return launch(h, ypipe_kernel<T>(My, By), ygrid, By * (My / 8), ypipe_smem<T>(My, By), s, spec,
-                          nkx, Mz, hxp, (const cplx<T>*)twy, inverse);
+            const int ntiles = ((k1 - k0 + By - 1) / By) * Mz * 3;
+            return launch(h, ypipe_kernel<T>(My, By), std::min(ygrid, ntiles), By * (My / 8), ypipe_smem<T>(My, By),
+                          s, spec, k0, k1, Mz, hxp, (const cplx<T>*)twy, inverse);
         }
         if (fast_y) {
-            dim3 g((nkx + By - 1) / By, Mz, 3);
+            dim3 g((k1 - k0 + By - 1) / By, Mz, 3);
             return launch(h, y_kernel<T>(My, By), g, By * (My / 8), FastFft<T>::yz_smem(My, By), s, spec,
-                          nkx, My, Mz, hxp, (const cplx<T>*)twy, inverse);
+                          k0, k1, My, Mz, hxp, (const cplx<T>*)twy, inverse);
         }
         dim3 gy((nkx + tx_y - 1) / tx_y, Mz, 3);
         return launch(h, k_fft_y<T>, gy, 256, smem_y, s, spec, nkx, My, Mz, hxp, plan_y,
                       (const cplx<T>*)twy, tx_y, inverse);
     }
 
-    int launch_z(cudaStream_t s) {
+    int launch_z(cudaStream_t s, int k0 = 0, int k1 = 0) {
+        if (k1 <= 0) k1 = nkx;
         if (fast_z && zkind == 1) {
-            return launch(h, zpipe_kernel<T>(Mz, Bz), zgrid, Bz * (Mz / 8), zpipe_smem<T>(Mz, Bz), s, spec,
-                          nkx, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+            const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
+            return launch(h, zpipe_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), zpipe_smem<T>(Mz, Bz),
+                          s, spec, k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
                           (const T*)kzv, inv_mu_M);
         }
         if (fast_z) {
-            dim3 g((nkx + Bz - 1) / Bz, My, 1);
+            dim3 g((k1 - k0 + Bz - 1) / Bz, My, 1);
             return launch(h, z_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::yz_smem(Mz, Bz), s, spec,
-                          nkx, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+                          k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
                           (const T*)kzv, inv_mu_M);
         }
         dim3 gz((nkx + tx_z - 1) / tx_z, My, 1);
@@ -924,18 +960,7 @@ struct Engine final : EngineBase {
             StageScope sc(h, FFCM_STAGE_FFT_X_FWD, s);
             TRY(x_forward(gf, s));
         }
-        {
-            StageScope sc(h, FFCM_STAGE_FFT_Y_FWD, s);
-            TRY(launch_y(s, 0));
-        }
-        {
-            StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
-            TRY(launch_z(s));
-        }
-        {
-            StageScope sc(h, FFCM_STAGE_FFT_Y_INV, s);
-            TRY(launch_y(s, 1));
-        }
+        TRY(stokes_yz(s));
         StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
         return x_inverse(out, s);
     }

@@ -22,9 +22,9 @@ struct FastFft {
 
 // Function-pointer tables for the y and z kernels, indexed by (n, B).
 template <typename T>
-using YKernel = void (*)(cplx<T>*, int, int, int, int, const cplx<T>*, int);
+using YKernel = void (*)(cplx<T>*, int, int, int, int, int, const cplx<T>*, int);
 template <typename T>
-using ZKernel = void (*)(cplx<T>*, int, int, int, const cplx<T>*, const T*, const T*, const T*, T);
+using ZKernel = void (*)(cplx<T>*, int, int, int, int, const cplx<T>*, const T*, const T*, const T*, T);
 template <typename T>
 using XfKernel = void (*)(const T*, cplx<T>*, int, int, const cplx<T>*, int);
 template <typename T>

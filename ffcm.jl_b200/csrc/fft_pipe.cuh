@@ -95,9 +95,10 @@ struct Chunks {
 };
 
 // ---- y pass: tiles of B kx columns x n rows of one (c, z) plane ------------
-// block = B * n/8 threads; smem: table (n) | staging (n * B) | exchange (B * padded_len(n)).
+// Columns kx0 <= kx < kx1 (kx0 a multiple of B). block = B * n/8 threads;
+// smem: table (n) | staging (n * B) | exchange (B * padded_len(n)).
 template <typename T, int n, int B>
-__global__ void __launch_bounds__(B * (n / 8)) k_fftq_y(cplx<T>* __restrict__ spec, int nkx, int Mz,
+__global__ void __launch_bounds__(B * (n / 8)) k_fftq_y(cplx<T>* __restrict__ spec, int kx0, int kx1, int Mz,
                                                         int hxp, const cplx<T>* __restrict__ twy,
                                                         int inverse) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -108,12 +109,12 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftq_y(cplx<T>* __restrict__ sp
     cplx<T>* ex_sm = stage + n * B;
     load_table(tw, twy, n);
     const int b = threadIdx.x % B, j = threadIdx.x / B;
-    const int tiles_x = (nkx + B - 1) / B;
+    const int tiles_x = (kx1 - kx0 + B - 1) / B;
     const int ntiles = tiles_x * Mz * 3;
     const int64_t plane_elems = (int64_t)n * hxp;
     auto issue = [&](int t) {
         const int tx = t % tiles_x, pz = t / tiles_x;   // pz = c * Mz + z
-        const cplx<T>* src = spec + (int64_t)pz * plane_elems + tx * B;
+        const cplx<T>* src = spec + (int64_t)pz * plane_elems + kx0 + tx * B;
         for (int q = threadIdx.x; q < n * CPR; q += NT) {
             const int y = q / CPR, part = q - y * CPR;
             cp_async16(reinterpret_cast<unsigned char*>(stage + y * B) + 16 * part,
@@ -134,8 +135,8 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftq_y(cplx<T>* __restrict__ sp
         if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
         fft_lines_lockstep<T, n, 1>(v, j, ex, tw, inverse != 0);
         const int tx = t % tiles_x, pz = t / tiles_x;
-        const int kx = tx * B + b;
-        if (kx < nkx) {
+        const int kx = kx0 + tx * B + b;
+        if (kx < kx1) {
             cplx<T>* dst = spec + (int64_t)pz * plane_elems + kx;
 #pragma unroll
             for (int q = 0; q < 8; ++q) dst[(int64_t)(j + q * Q) * hxp] = v[0][q];
@@ -144,10 +145,11 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftq_y(cplx<T>* __restrict__ sp
 }
 
 // ---- z pass + projector: tiles of B kx columns x n z of one y, 3 components --
-// block = B * n/8 threads; smem: table (n) | staging (3 n B) | exchange (3 B padded_len(n)).
+// Columns kx0 <= kx < kx1 (kx0 a multiple of B). block = B * n/8 threads;
+// smem: table (n) | staging (3 n B) | exchange (3 B padded_len(n)).
 template <typename T, int n, int B>
 __global__ void __launch_bounds__(B * (n / 8)) k_fftq_z_stokes(
-    cplx<T>* __restrict__ spec, int nkx, int My, int hxp, const cplx<T>* __restrict__ twz,
+    cplx<T>* __restrict__ spec, int kx0, int kx1, int My, int hxp, const cplx<T>* __restrict__ twz,
     const T* __restrict__ kxv, const T* __restrict__ kyv, const T* __restrict__ kzv, T inv_mu_M) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int Q = n / 8, CPR = Chunks<T, B>::PER_ROW;
@@ -158,13 +160,13 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftq_z_stokes(
     cplx<T>* ex_sm = stage + 3 * n * B;
     load_table(tw, twz, n);
     const int b = threadIdx.x % B, j = threadIdx.x / B;
-    const int tiles_x = (nkx + B - 1) / B;
+    const int tiles_x = (kx1 - kx0 + B - 1) / B;
     const int ntiles = tiles_x * My;
     const int64_t zs = (int64_t)My * hxp;
     const int64_t cs = (int64_t)n * zs;
     auto issue = [&](int t) {
         const int tx = t % tiles_x, y = t / tiles_x;
-        const cplx<T>* src = spec + (int64_t)y * hxp + tx * B;
+        const cplx<T>* src = spec + (int64_t)y * hxp + kx0 + tx * B;
         for (int q = threadIdx.x; q < 3 * n * CPR; q += NT) {
             const int row = q / CPR, part = q - row * CPR;   // row = c * n + z
             const int c = row / n, z = row - c * n;
@@ -188,9 +190,9 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftq_z_stokes(
         __syncthreads();
         if (t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
         const int tx = t % tiles_x, y = t / tiles_x;
-        const int kx = tx * B + b;
+        const int kx = kx0 + tx * B + b;
         fft_lines_lockstep<T, n, 3>(v, j, ex, tw, false);
-        const T k1 = kx < nkx ? kxv[kx] : T(0);
+        const T k1 = kx < kx1 ? kxv[kx] : T(0);
         const T k2 = kyv[y];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -209,7 +211,7 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftq_z_stokes(
             }
         }
         fft_lines_lockstep<T, n, 3>(v, j, ex, tw, true);
-        if (kx < nkx) {
+        if (kx < kx1) {
             cplx<T>* col = spec + (int64_t)y * hxp + kx;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
@@ -223,9 +225,9 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftq_z_stokes(
 }
 
 template <typename T>
-using YPipeKernel = void (*)(cplx<T>*, int, int, int, const cplx<T>*, int);
+using YPipeKernel = void (*)(cplx<T>*, int, int, int, int, const cplx<T>*, int);
 template <typename T>
-using ZPipeKernel = void (*)(cplx<T>*, int, int, int, const cplx<T>*, const T*, const T*, const T*, T);
+using ZPipeKernel = void (*)(cplx<T>*, int, int, int, int, const cplx<T>*, const T*, const T*, const T*, T);
 
 template <typename T>
 size_t ypipe_smem(int n, int B) {

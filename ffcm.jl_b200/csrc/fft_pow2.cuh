@@ -50,10 +50,13 @@ struct Exchange {
 
 // In-register FFT of one line: v[q] = x[j + q n/8] on entry, X[j + q n/8] on exit.
 // `tw` holds W_n^t for t = e * tws (tws = table stride). All threads of the
-// block must call this together (it contains __syncthreads()).
-template <typename T, int n>
+// block must call this together (it contains __syncthreads()). With
+// WARP = true every line lies inside one warp (n/8 <= 32 consecutive threads,
+// lines not shared between warps) and the exchanges only synchronise the warp.
+template <typename T, int n, bool WARP = false>
 __device__ __forceinline__ void fft_line_regs(cplx<T> (&v)[8], int j, const Exchange<T>& ex,
                                               const cplx<T>* tw, int tws, bool inv) {
+    static_assert(!WARP || n / 8 <= 32, "a warp-synchronised line must fit in one warp");
     constexpr int L2 = ilog2c(n);
     constexpr int NR8 = L2 / 3;
     constexpr int RL = 1 << (L2 % 3);
@@ -70,10 +73,10 @@ __device__ __forceinline__ void fft_line_regs(cplx<T> (&v)[8], int j, const Exch
         dft8(v, inv);
         if (s < NR8 - 1 || RL > 1) {
             const int o = (j / Ns) * 8 * Ns + (j & (Ns - 1));
-            __syncthreads();
+            if (WARP) __syncwarp(); else __syncthreads();
 #pragma unroll
             for (int r = 0; r < 8; ++r) ex.at(o + r * Ns) = v[r];
-            __syncthreads();
+            if (WARP) __syncwarp(); else __syncthreads();
 #pragma unroll
             for (int q = 0; q < 8; ++q) v[q] = ex.at(j + q * Q);
         }
@@ -125,12 +128,14 @@ __global__ void __launch_bounds__(256) k_fftp_x_r2c(const T* __restrict__ f, cpl
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = active ? src[j + q * Q] : cplx<T>{T(0), T(0)};
     __syncthreads();  // table ready
+    // each line owns its exchange slot; a line inside one warp syncs the warp only
+    constexpr bool WARP = TPL <= 32;
     Exchange<T> ex{ex_sm, b * padded_len(H), 1};
-    fft_line_regs<T, H>(v, j, ex, tw, 2, false);
-    __syncthreads();
+    fft_line_regs<T, H, WARP>(v, j, ex, tw, 2, false);
+    if (WARP) __syncwarp(); else __syncthreads();
 #pragma unroll
     for (int q = 0; q < 8; ++q) ex.at(j + q * Q) = v[q];
-    __syncthreads();
+    if (WARP) __syncwarp(); else __syncthreads();
     if (!active) return;
     cplx<T>* dst = spec + (int64_t)row * hxp;
 #pragma unroll
@@ -178,7 +183,7 @@ __global__ void __launch_bounds__(256) k_fftp_x_c2r(const cplx<T>* __restrict__ 
         v[q] = cadd(A, mul_pi(B));
     }
     Exchange<T> ex{ex_sm, b * padded_len(H), 1};
-    fft_line_regs<T, H>(v, j, ex, tw, 2, true);
+    fft_line_regs<T, H, (TPL <= 32)>(v, j, ex, tw, 2, true);
     if (!active) return;
     cplx<T>* dst = reinterpret_cast<cplx<T>*>(u + (int64_t)row * Mx);
 #pragma unroll
@@ -186,9 +191,10 @@ __global__ void __launch_bounds__(256) k_fftp_x_c2r(const cplx<T>* __restrict__ 
 }
 
 // ---- passes 2 and 4: y, B consecutive kx columns of one (c, z) plane -------
+// Columns kx0 <= kx < kx1 (a chunk of the spectrum; grid.x covers it).
 // block = B * (n/8) threads, b fastest; smem: table (n) + B * padded_len(n).
 template <typename T, int n, int B>
-__global__ void __launch_bounds__(B * (n / 8)) k_fftp_y(cplx<T>* __restrict__ spec, int nkx, int My,
+__global__ void __launch_bounds__(B * (n / 8)) k_fftp_y(cplx<T>* __restrict__ spec, int kx0, int kx1, int My,
                                                         int Mz, int hxp, const cplx<T>* __restrict__ twy,
                                                         int inverse) {
     extern __shared__ unsigned char smem_raw[];
@@ -197,8 +203,8 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftp_y(cplx<T>* __restrict__ sp
     cplx<T>* ex_sm = tw + n;
     load_table(tw, twy, n);
     const int b = threadIdx.x % B, j = threadIdx.x / B;
-    const int kx = blockIdx.x * B + b;
-    const bool active = kx < nkx;
+    const int kx = kx0 + blockIdx.x * B + b;
+    const bool active = kx < kx1;
     cplx<T>* plane = spec + ((int64_t)blockIdx.z * Mz + blockIdx.y) * My * hxp + (active ? kx : 0);
     cplx<T> v[8];
 #pragma unroll
@@ -214,7 +220,7 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftp_y(cplx<T>* __restrict__ sp
 // ---- pass 3: z forward, projector, z inverse; B kx columns of one y -------
 template <typename T, int n, int B>
 __global__ void __launch_bounds__(B * (n / 8)) k_fftp_z_stokes(
-    cplx<T>* __restrict__ spec, int nkx, int My, int hxp, const cplx<T>* __restrict__ twz,
+    cplx<T>* __restrict__ spec, int kx0, int kx1, int My, int hxp, const cplx<T>* __restrict__ twz,
     const T* __restrict__ kxv, const T* __restrict__ kyv, const T* __restrict__ kzv, T inv_mu_M) {
     extern __shared__ unsigned char smem_raw[];
     constexpr int Q = n / 8;
@@ -222,9 +228,9 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftp_z_stokes(
     cplx<T>* ex_sm = tw + n;
     load_table(tw, twz, n);
     const int b = threadIdx.x % B, j = threadIdx.x / B;
-    const int kx = blockIdx.x * B + b;
+    const int kx = kx0 + blockIdx.x * B + b;
     const int y = blockIdx.y;
-    const bool active = kx < nkx;
+    const bool active = kx < kx1;
     const int64_t zs = (int64_t)My * hxp;
     const int64_t cs = (int64_t)n * zs;
     cplx<T>* col = spec + (int64_t)y * hxp + (active ? kx : 0);

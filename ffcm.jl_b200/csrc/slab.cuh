@@ -329,28 +329,19 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
     slab_scan<T, BY, BZ, H, true>(
         Ys, Fs, off, p, g, y0r, z0r, W, lists + (int64_t)cta * g.lcap, counts + cta, [&](int count) {
             __syncthreads();
+            // sort the window by first x point: each entry's rank is the
+            // number of entries with a smaller (key, index) pair
             for (int i = threadIdx.x; i < SLAB_CAP; i += blockDim.x) {
                 if (i < count) {
                     slab_entry_weights(p, W, i, y0r, z0r);
-                    W.sk[i] = ((unsigned)W.key[i] << 7) | (unsigned)i;
+                    const unsigned me = ((unsigned)W.key[i] << 7) | (unsigned)i;
+                    int rank = 0;
+                    for (int k = 0; k < count; ++k) rank += (((unsigned)W.key[k] << 7) | (unsigned)k) < me;
+                    W.sk[rank] = me;
                 } else {
                     W.sk[i] = 0xffffffffu;
                 }
             }
-            // bitonic sort of the window by first x point
-            for (int k = 2; k <= SLAB_CAP; k <<= 1)
-                for (int j = k >> 1; j > 0; j >>= 1) {
-                    __syncthreads();
-                    const int t = threadIdx.x;
-                    if (t < SLAB_CAP / 2) {
-                        const int a = 2 * j * (t / j) + (t % j), b = a + j;
-                        const unsigned va = W.sk[a], vb = W.sk[b];
-                        if ((va > vb) == ((a & k) == 0)) {
-                            W.sk[a] = vb;
-                            W.sk[b] = va;
-                        }
-                    }
-                }
             __syncthreads();
             for (int v = threadIdx.x; v <= Mx; v += blockDim.x) {
                 int lo = 0, hi = SLAB_CAP;   // first sorted entry with key >= v
@@ -408,10 +399,15 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
                     for (int r = 0; r < NRP; ++r) acc[(c * NRP + r) * P + x] += a[c][r];
             }
         });
-    // x r2c of every slab row (H/8 threads per row), output straight to spec
+    // x r2c of every slab row (H/8 threads per row), output straight to spec.
+    // A row that fits one warp is transformed with warp-level synchronisation
+    // only (rows are disjoint between warps; idle lanes exchange through a
+    // scratch line whose contents are never used).
     constexpr int TPL = H / 8, Q = H / 8;
+    constexpr bool WARP = TPL <= 32;
     const int lines_per_round = blockDim.x / TPL;
     const int lr = threadIdx.x / TPL, j = threadIdx.x - lr * TPL;
+    __syncthreads();
     for (int r0 = 0; r0 < ROWS; r0 += lines_per_round) {
         const int r = r0 + lr;
         const bool active = r < ROWS && lr < lines_per_round;
@@ -420,13 +416,13 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
 #pragma unroll
         for (int qq = 0; qq < 8; ++qq) v[qq] = active ? rowc[j + qq * Q] : cplx<T>{T(0), T(0)};
         Exchange<T> ex{active ? rowc : dummy, 0, 1};
-        fft_line_regs<T, H>(v, j, ex, tw, 2, false);
-        __syncthreads();
+        fft_line_regs<T, H, WARP>(v, j, ex, tw, 2, false);
+        if (WARP) __syncwarp(); else __syncthreads();
         if (active) {
 #pragma unroll
             for (int qq = 0; qq < 8; ++qq) ex.at(j + qq * Q) = v[qq];
         }
-        __syncthreads();
+        if (WARP) __syncwarp(); else __syncthreads();
         if (active) {
             const int c = r / NRP, bd = r % NRP;
             const int b = bd % BY, d = bd / BY;
@@ -444,7 +440,7 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
                 dst[H] = cplx<T>{Z0.x - Z0.y, T(0)};
             }
         }
-        __syncthreads();
+        if (WARP) __syncwarp(); else __syncthreads();
     }
 }
 
@@ -470,6 +466,7 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
     load_table(tw, twx, Mx);
     __syncthreads();
     constexpr int TPL = H / 8, Q = H / 8;
+    constexpr bool WARP = TPL <= 32;
     const int lines_per_round = blockDim.x / TPL;
     const int lr = threadIdx.x / TPL, j = threadIdx.x - lr * TPL;
     for (int r0 = 0; r0 < ROWS; r0 += lines_per_round) {
@@ -494,14 +491,15 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
         }
         cplx<T>* rowc = reinterpret_cast<cplx<T>*>(acc + (active ? r : 0) * P);
         Exchange<T> ex{active ? rowc : dummy, 0, 1};
-        fft_line_regs<T, H>(v, j, ex, tw, 2, true);
-        __syncthreads();
+        fft_line_regs<T, H, WARP>(v, j, ex, tw, 2, true);
+        if (WARP) __syncwarp(); else __syncthreads();
         if (active) {
 #pragma unroll
             for (int qq = 0; qq < 8; ++qq) rowc[j + qq * Q] = v[qq];   // real row, unpadded
         }
-        __syncthreads();
+        if (WARP) __syncwarp(); else __syncthreads();
     }
+    __syncthreads();
     auto gather = [&](int count) {
         for (int i = threadIdx.x; i < count; i += blockDim.x) {
             slab_entry_weights(p, W, i, y0r, z0r);
