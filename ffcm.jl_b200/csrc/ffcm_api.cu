@@ -744,10 +744,13 @@ struct Engine final : EngineBase {
 
     int spread_to_spectrum(cudaStream_t s, const vec4<T>* force = nullptr) {
         StageScope sc(h, FFCM_STAGE_SPREAD, s);
+        const int nslab = sg.nty * sg.ntz;
+        TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
+                   slab_lists, slab_counts));
         dim3 g(sg.nty, sg.ntz, 1);
         return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys, force ? force : (const vec4<T>*)Fs,
-                      (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, slab_lists,
-                      slab_counts);
+                      (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, (const int*)slab_lists,
+                      (const int*)slab_counts);
     }
 
     // y forward, z + projector, y inverse. With kx chunking (kx_chunk > 0) the

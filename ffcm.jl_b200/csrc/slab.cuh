@@ -96,8 +96,10 @@ struct SlabWin {
     unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15)
     T y0[SLAB_CAP], y1[SLAB_CAP], y2[SLAB_CAP];
     T f[3][SLAB_CAP];
-    T gx[SLAB_CAP][SLAB_MG], r2x[SLAB_CAP][SLAB_MG];
-    T gyz[SLAB_CAP][NRP], r2yz[SLAB_CAP][NRP];
+    // rows padded by one element: lanes reading different entries at the same
+    // stencil point or slab row then fall into different banks
+    T gx[SLAB_CAP][SLAB_MG + 1], r2x[SLAB_CAP][SLAB_MG + 1];
+    T gyz[SLAB_CAP][NRP + 1], r2yz[SLAB_CAP][NRP + 1];
     unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry)
     int first[2 * H + 1];     // first sorted entry with key >= v
     int pair_start[SLAB_PAIRMAX + 1];
@@ -284,12 +286,13 @@ __device__ __forceinline__ void slab_scan(const vec4<T>* __restrict__ Ys, const 
     __syncthreads();
 }
 
-// Replay a stored slab list in windows (the interpolation's path when the
-// spread kept the list).
-template <typename T, int BY, int BZ, int H, typename Process>
-__device__ __forceinline__ void slab_replay(const vec4<T>* __restrict__ Ys, const StencilParams<T>& p,
-                                           int y0r, int z0r, SlabWin<T, BY, BZ, H>& W,
-                                           const int* __restrict__ glist, int total, Process&& process) {
+// Replay a stored slab list in windows of SLAB_CAP entries (the list holds
+// only particles that touch the slab, in candidate order).
+template <typename T, int BY, int BZ, int H, bool WANT_F, typename Process>
+__device__ __forceinline__ void slab_replay(const vec4<T>* __restrict__ Ys, const vec4<T>* __restrict__ Fs,
+                                           const StencilParams<T>& p, int y0r, int z0r,
+                                           SlabWin<T, BY, BZ, H>& W, const int* __restrict__ glist, int total,
+                                           Process&& process) {
     for (int w0 = 0; w0 < total; w0 += SLAB_CAP) {
         const int n = min(SLAB_CAP, total - w0);
         if ((int)threadIdx.x < n) {
@@ -299,11 +302,60 @@ __device__ __forceinline__ void slab_replay(const vec4<T>* __restrict__ Ys, cons
             unsigned m;
             slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
             slab_put(W, (int)threadIdx.x, s, y, sx, sy, sz, m);
+            if (WANT_F) {
+                const vec4<T> f = Fs[s];
+                W.f[0][threadIdx.x] = f.x;
+                W.f[1][threadIdx.x] = f.y;
+                W.f[2][threadIdx.x] = f.z;
+            }
         }
         __syncthreads();
         process(n);
         __syncthreads();
     }
+}
+
+// Per-slab particle lists, one warp per slab: the candidates (particles of
+// the slab's cell rows, in sorted order) are tested with the same integer
+// anchor arithmetic as the slab kernels and the touching ones appended, in
+// candidate order, with a warp ballot. lists[slab][0, lcap), counts[slab]
+// (-1 when the list did not fit; the slab kernels then scan for themselves).
+template <typename T, int BY, int BZ>
+__global__ void k_slab_lists(const vec4<T>* __restrict__ Ys, const int32_t* __restrict__ off,
+                             StencilParams<T> p, SlabGeom g, int* __restrict__ lists, int* __restrict__ counts) {
+    constexpr int half = SLAB_MG / 2;
+    const int lane = threadIdx.x & 31;
+    const int slab = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (slab >= g.nty * g.ntz) return;   // whole warps leave together
+    const int ty = slab % g.nty, tz = slab / g.nty;
+    const int y0r = ty * BY, z0r = tz * BZ;
+    int cy_lo, ny, cz_lo, nz;
+    cell_span(y0r - SLAB_MG + 1 + half, y0r + BY - 1 + half, g.h, g.cs1, g.m1, cy_lo, ny);
+    cell_span(z0r - SLAB_MG + 1 + half, z0r + BZ - 1 + half, g.h, g.cs2, g.m2, cz_lo, nz);
+    int* out = lists + (int64_t)slab * g.lcap;
+    const unsigned lt = (1u << lane) - 1u;
+    int total = 0;
+    for (int pi = 0; pi < ny * nz; ++pi) {
+        const int cy = imod(cy_lo + pi % ny, g.m1);
+        const int cz = imod(cz_lo + pi / ny, g.m2);
+        const int c0 = (cy + cz * g.m1) * g.m0;
+        const int sb = off[c0], se = off[c0 + g.m0];
+        for (int b = sb; b < se; b += 32) {
+            const int s = b + lane;
+            unsigned m = 0;
+            if (s < se) {
+                int sx, sy, sz;
+                slab_anchor<T, BY, BZ>(p, Ys[s], y0r, z0r, sx, sy, sz, m);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, m != 0);
+            if (m) {
+                const int pos = total + __popc(bal & lt);
+                if (pos < g.lcap) out[pos] = s;
+            }
+            total += __popc(bal);
+        }
+    }
+    if (lane == 0) counts[slab] = total <= g.lcap ? total : -1;
 }
 
 // ---- spread into a slab, then x-r2c straight into the spectrum -----------
@@ -314,7 +366,8 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
                                                      cplx<T>* __restrict__ spec, int hxp,
                                                      StencilParams<T> p, SlabGeom g,
                                                      const cplx<T>* __restrict__ twx,
-                                                     int* __restrict__ lists, int* __restrict__ counts) {
+                                                     const int* __restrict__ lists,
+                                                     const int* __restrict__ counts) {
     constexpr int Mx = 2 * H, P = slab_pitch(Mx), NRP = BY * BZ, ROWS = 3 * NRP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
@@ -326,8 +379,7 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
     for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
     load_table(tw, twx, Mx);
     __syncthreads();
-    slab_scan<T, BY, BZ, H, true>(
-        Ys, Fs, off, p, g, y0r, z0r, W, lists + (int64_t)cta * g.lcap, counts + cta, [&](int count) {
+    auto process = [&](int count) {
             __syncthreads();
             // sort the window by first x point: each entry's rank is the
             // number of entries with a smaller (key, index) pair
@@ -398,7 +450,13 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
 #pragma unroll
                     for (int r = 0; r < NRP; ++r) acc[(c * NRP + r) * P + x] += a[c][r];
             }
-        });
+        };
+    const int stored = counts[cta];
+    if (stored >= 0) {
+        slab_replay<T, BY, BZ, H, true>(Ys, Fs, p, y0r, z0r, W, lists + (int64_t)cta * g.lcap, stored, process);
+    } else {
+        slab_scan<T, BY, BZ, H, true>(Ys, Fs, off, p, g, y0r, z0r, W, nullptr, nullptr, process);
+    }
     // x r2c of every slab row (H/8 threads per row), output straight to spec.
     // A row that fits one warp is transformed with warp-level synchronisation
     // only (rows are disjoint between warps; idle lanes exchange through a
@@ -532,7 +590,7 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
     };
     const int stored = counts[cta];
     if (stored >= 0) {
-        slab_replay<T, BY, BZ, H>(Ys, p, y0r, z0r, W, lists + (int64_t)cta * g.lcap, stored, gather);
+        slab_replay<T, BY, BZ, H, false>(Ys, nullptr, p, y0r, z0r, W, lists + (int64_t)cta * g.lcap, stored, gather);
     } else {
         slab_scan<T, BY, BZ, H, false>(Ys, nullptr, off, p, g, y0r, z0r, W, nullptr, nullptr,
                                       [&](int count) {
@@ -545,7 +603,9 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
 // ---- host-side dispatch over the x length ----------------------------------
 template <typename T>
 using SpreadSlabKernel = void (*)(const vec4<T>*, const vec4<T>*, const int32_t*, cplx<T>*, int,
-                                  StencilParams<T>, SlabGeom, const cplx<T>*, int*, int*);
+                                  StencilParams<T>, SlabGeom, const cplx<T>*, const int*, const int*);
+template <typename T>
+using ListsKernel = void (*)(const vec4<T>*, const int32_t*, StencilParams<T>, SlabGeom, int*, int*);
 template <typename T>
 using InterpSlabKernel = void (*)(const vec4<T>*, const int32_t*, const cplx<T>*, int, T*,
                                   StencilParams<T>, SlabGeom, const cplx<T>*, const int*, const int*);
@@ -554,6 +614,7 @@ template <typename T>
 struct SlabKernels {
     SpreadSlabKernel<T> spread_fused = nullptr;
     InterpSlabKernel<T> interp = nullptr;
+    ListsKernel<T> lists = nullptr;
     int BY = 0, BZ = 0;
     size_t smem = 0;
 };
@@ -564,6 +625,7 @@ SlabKernels<T> slab_kernels_for() {
     SlabKernels<T> k;
     k.spread_fused = k_spread_slab<T, H, BY, BZ>;
     k.interp = k_interp_slab<T, H, BY, BZ>;
+    k.lists = k_slab_lists<T, BY, BZ>;
     k.BY = BY;
     k.BZ = BZ;
     k.smem = (size_t)3 * BY * BZ * slab_pitch(2 * H) * sizeof(T) +
