@@ -474,7 +474,7 @@ struct Engine final : EngineBase {
             sg.lcap = (int)std::min<double>(1 << 20, std::max(256.0, 4.0 * expect + 64.0));
             sg.lcap = (sg.lcap + 31) / 32 * 32;
             TRY(raise_smem_cap((const void*)sk.spread_fused, sk.smem));
-            TRY(raise_smem_cap((const void*)sk.interp, sk.smem));
+            TRY(raise_smem_cap((const void*)sk.interp, sk.smem_interp));
         }
         if (fast_y) {
             int cand[4];
@@ -498,6 +498,8 @@ struct Engine final : EngineBase {
         for (int B : {2, 4, 8, 16}) {
             if (fast_y && ypipe_kernel<T>(My, B) && hxp % B == 0 && ypipe_smem<T>(My, B) <= budget)
                 TRY(raise_smem_cap((const void*)ypipe_kernel<T>(My, B), ypipe_smem<T>(My, B)));
+            if (fast_z && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= budget)
+                TRY(raise_smem_cap((const void*)zlr_kernel<T>(Mz, B), FastFft<T>::zlr_smem(Mz, B)));
             if (fast_z && zpipe_kernel<T>(Mz, B) && hxp % B == 0 && zpipe_smem<T>(Mz, B) <= budget)
                 TRY(raise_smem_cap((const void*)zpipe_kernel<T>(Mz, B), zpipe_smem<T>(Mz, B)));
         }
@@ -644,11 +646,12 @@ struct Engine final : EngineBase {
         if (fast_z) {
             float best = 1e30f;
             int bk = 0, bB = Bz, bg = 0;
-            for (int kind = 0; kind < 2; ++kind)
+            for (int kind = 0; kind < 3; ++kind)
                 for (int B : {2, 4, 8, 16}) {
                     if (kind == 0 && !z_kernel<T>(Mz, B)) continue;
                     if (kind == 1 && !(zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
                                        zpipe_smem<T>(Mz, B) <= 200 * 1024)) continue;
+                    if (kind == 2 && !(zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= 200 * 1024)) continue;
                     if (kind == 0) {
                         int cand[4];
                         const int nc = z_bundles(Mz, cand);
@@ -785,7 +788,7 @@ struct Engine final : EngineBase {
         StageScope sc(h, FFCM_STAGE_INTERPOLATE, s);
         CUDA_TRY(cudaMemsetAsync(partial, 0, 3 * (size_t)N * sizeof(T), s));
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, sk.interp, g, 256, sk.smem, s, (const vec4<T>*)Ys, (const int32_t*)off,
+        return launch(h, sk.interp, g, 256, sk.smem_interp, s, (const vec4<T>*)Ys, (const int32_t*)off,
                       (const cplx<T>*)spec, hxp, partial, sp, sg, (const cplx<T>*)twx,
                       (const int*)slab_lists, (const int*)slab_counts);
     }
@@ -913,6 +916,12 @@ struct Engine final : EngineBase {
 
     int launch_z(cudaStream_t s, int k0 = 0, int k1 = 0) {
         if (k1 <= 0) k1 = nkx;
+        if (fast_z && zkind == 2) {
+            dim3 g((k1 - k0 + Bz - 1) / Bz, My, 1);
+            return launch(h, zlr_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::zlr_smem(Mz, Bz), s, spec,
+                          k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+                          (const T*)kzv, inv_mu_M);
+        }
         if (fast_z && zkind == 1) {
             const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
             return launch(h, zpipe_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), zpipe_smem<T>(Mz, Bz),

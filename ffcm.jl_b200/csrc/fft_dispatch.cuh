@@ -18,6 +18,7 @@ struct FastFft {
         return (size_t)(2 * H + x_lpb(H) * padded_len(H)) * sizeof(cplx<T>);
     }
     static size_t yz_smem(int n, int B) { return (size_t)(n + B * padded_len(n)) * sizeof(cplx<T>); }
+    static size_t zlr_smem(int n, int B) { return (size_t)(n + 3 * B * padded_len(n)) * sizeof(cplx<T>); }
 };
 
 // Function-pointer tables for the y and z kernels, indexed by (n, B).
@@ -45,6 +46,15 @@ ZKernel<T> z_kernel(int n, int B) {
     FFCM_Z(32, 8) FFCM_Z(32, 16) FFCM_Z(64, 8) FFCM_Z(64, 16) FFCM_Z(128, 4) FFCM_Z(128, 8)
     FFCM_Z(256, 4) FFCM_Z(256, 8) FFCM_Z(512, 4) FFCM_Z(512, 8) FFCM_Z(1024, 2) FFCM_Z(1024, 4)
 #undef FFCM_Z
+    return nullptr;
+}
+
+template <typename T>
+ZKernel<T> zlr_kernel(int n, int B) {
+#define FFCM_ZL(NN, BB) if (n == NN && B == BB) return k_fftp_z_stokes_lr<T, NN, BB>;
+    FFCM_ZL(64, 8) FFCM_ZL(64, 16) FFCM_ZL(128, 4) FFCM_ZL(128, 8) FFCM_ZL(256, 2) FFCM_ZL(256, 4)
+    FFCM_ZL(256, 8) FFCM_ZL(512, 2) FFCM_ZL(512, 4) FFCM_ZL(1024, 2)
+#undef FFCM_ZL
     return nullptr;
 }
 

@@ -278,4 +278,78 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftp_z_stokes(
     }
 }
 
+// ---- pass 3, low-register variant --------------------------------------
+// Same result as k_fftp_z_stokes; the three components go through the
+// forward transform one after the other and wait in shared memory for the
+// projector, then each is inverse-transformed from there. One line of 8
+// values per thread is live at a time, so more blocks fit on an SM.
+// block = B * (n/8) threads, b fastest; smem: table (n) + 3 * B * padded_len(n).
+template <typename T, int n, int B>
+__global__ void __launch_bounds__(B * (n / 8), (768 / (B * (n / 8))) > 0 ? 768 / (B * (n / 8)) : 1)
+    k_fftp_z_stokes_lr(
+    cplx<T>* __restrict__ spec, int kx0, int kx1, int My, int hxp, const cplx<T>* __restrict__ twz,
+    const T* __restrict__ kxv, const T* __restrict__ kyv, const T* __restrict__ kzv, T inv_mu_M) {
+    extern __shared__ unsigned char smem_raw[];
+    constexpr int Q = n / 8, PL = padded_len(n);
+    cplx<T>* tw = reinterpret_cast<cplx<T>*>(smem_raw);
+    cplx<T>* ex_sm = tw + n;
+    load_table(tw, twz, n);
+    const int b = threadIdx.x % B, j = threadIdx.x / B;
+    const int kx = kx0 + blockIdx.x * B + b;
+    const int y = blockIdx.y;
+    const bool active = kx < kx1;
+    const int64_t zs = (int64_t)My * hxp;
+    const int64_t cs = (int64_t)n * zs;
+    cplx<T>* col = spec + (int64_t)y * hxp + (active ? kx : 0);
+    const Exchange<T> ex[3] = {Exchange<T>{ex_sm, b, B}, Exchange<T>{ex_sm + B * PL, b, B},
+                               Exchange<T>{ex_sm + 2 * B * PL, b, B}};
+    __syncthreads();  // table ready
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+        cplx<T> v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            v[q] = active ? col[c * cs + (int64_t)(j + q * Q) * zs] : cplx<T>{T(0), T(0)};
+        fft_line_regs<T, n>(v, j, ex[c], tw, 1, false);
+        __syncthreads();   // the line's last exchange has been read
+#pragma unroll
+        for (int q = 0; q < 8; ++q) ex[c].at(j + q * Q) = v[q];
+    }
+    // projector at this thread's points (its own slots of the three lines)
+    const T k1 = active ? kxv[kx] : T(0);
+    const T k2 = kyv[y];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int z = j + q * Q;
+        const T k3 = kzv[z];
+        const T ksq = k1 * k1 + k2 * k2 + k3 * k3;
+        cplx<T> a0 = ex[0].at(z), a1 = ex[1].at(z), a2 = ex[2].at(z);
+        if (ksq == T(0)) {
+            a0 = a1 = a2 = cplx<T>{T(0), T(0)};
+        } else {
+            const T inv_k2 = T(1) / ksq;
+            const T sc = inv_mu_M * inv_k2;
+            const T dre = (k1 * a0.x + k2 * a1.x + k3 * a2.x) * inv_k2;
+            const T dim = (k1 * a0.y + k2 * a1.y + k3 * a2.y) * inv_k2;
+            a0 = cplx<T>{sc * (a0.x - k1 * dre), sc * (a0.y - k1 * dim)};
+            a1 = cplx<T>{sc * (a1.x - k2 * dre), sc * (a1.y - k2 * dim)};
+            a2 = cplx<T>{sc * (a2.x - k3 * dre), sc * (a2.y - k3 * dim)};
+        }
+        ex[0].at(z) = a0;
+        ex[1].at(z) = a1;
+        ex[2].at(z) = a2;
+    }
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+        cplx<T> v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = ex[c].at(j + q * Q);
+        fft_line_regs<T, n>(v, j, ex[c], tw, 1, true);
+        if (active) {
+#pragma unroll
+            for (int q = 0; q < 8; ++q) col[c * cs + (int64_t)(j + q * Q) * zs] = v[q];
+        }
+    }
+}
+
 }  // namespace ffcm

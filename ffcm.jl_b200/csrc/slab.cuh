@@ -4,24 +4,27 @@
 //
 // A block owns a slab: BY x BZ full x-rows of the grid, all three components,
 // held in shared memory. The particles whose stencil can touch the slab are
-// the particles of a few (cy, cz) rows of cells, each row one contiguous range
-// of the cell-sorted order; the block scans them and keeps those that touch
-// (integer anchor arithmetic, as the reference computes it), in candidate
-// order, in windows of SLAB_CAP entries.
+// listed once per solve by k_slab_lists (one warp per slab, over the few
+// (cy, cz) rows of cells that can reach it, in cell-sorted order, with the
+// reference's integer anchor arithmetic).
 //
-//  * k_spread_slab: per window, one thread per entry computes the separable
-//    weights (src/stencil.jl:80-112); the entries are sorted by the first x
-//    point of their stencil, and each thread then owns grid points x and
-//    gathers F (a0 + a2 r^2) gx gy gz from the entries covering x into
-//    registers (src/spread_forces.jl:73-130) — no atomics, deterministic.
-//    Each slab row is then x-r2c transformed in shared memory and written
-//    straight to the spectrum. The block also stores its particle list, so
-//    the interpolation does not scan again.
+//  * k_spread_slab: the list is replayed in windows of SLAB_CAP entries; one
+//    thread per entry stores the entry's per-row weights gy gz and r^2 parts
+//    (src/stencil.jl:80-112); the window is ordered by the first x point of
+//    each stencil, and each thread then owns grid points x and gathers
+//    F (a0 + a2 r^2) gx gy gz from the entries covering x into registers
+//    (src/spread_forces.jl:73-130; gx is evaluated by the one thread that
+//    uses it) — no atomics, deterministic. Each slab row is then x-r2c
+//    transformed in shared memory and written straight to the spectrum.
 //  * k_interp_slab: the slab's spectrum rows are x-c2r transformed into shared
 //    memory; one thread per listed particle gathers its partial velocity over
-//    the slab rows (src/interpolate.jl:322-376) and adds it, with an L2
-//    reduction, to a sorted-order velocity buffer that the correction kernel
-//    finishes (h^3 scale, correction, scatter to the caller's order).
+//    the slab rows from registers (src/interpolate.jl:322-376) and adds it,
+//    with an L2 reduction, to a sorted-order velocity buffer that the
+//    correction kernel finishes (h^3 scale, correction, scatter to the
+//    caller's order).
+//
+// A slab whose list did not fit its capacity is scanned by the slab kernel
+// itself (same candidates, same order).
 #pragma once
 
 #include "common.cuh"
@@ -31,7 +34,7 @@
 namespace ffcm {
 
 constexpr int SLAB_MG = 8;        // stencil width of the fused path
-constexpr int SLAB_CAP = 128;     // entries per list window (shared memory)
+constexpr int SLAB_CAP = 128;     // entries per spread window (shared memory)
 constexpr int SLAB_PAIRMAX = 512; // cell rows one slab may scan
 
 struct SlabGeom {
@@ -72,6 +75,27 @@ __device__ __forceinline__ void cell_span(int lo_anchor, int hi_anchor, double h
     }
 }
 
+// The (cy, cz) cell rows a slab's candidates come from.
+struct SlabRows {
+    int cy_lo, ny, cz_lo, nz;
+};
+
+template <int BY, int BZ>
+__device__ __forceinline__ SlabRows slab_rows(const SlabGeom& g, int y0r, int z0r) {
+    constexpr int half = SLAB_MG / 2;
+    SlabRows r;
+    cell_span(y0r - SLAB_MG + 1 + half, y0r + BY - 1 + half, g.h, g.cs1, g.m1, r.cy_lo, r.ny);
+    cell_span(z0r - SLAB_MG + 1 + half, z0r + BZ - 1 + half, g.h, g.cs2, g.m2, r.cz_lo, r.nz);
+    return r;
+}
+
+// First cell of cell row pi (x = 0), pi = iy + ny * iz.
+__device__ __forceinline__ int slab_row_cell(const SlabGeom& g, const SlabRows& r, int pi) {
+    const int cy = imod(r.cy_lo + pi % r.ny, g.m1);
+    const int cz = imod(r.cz_lo + pi / r.ny, g.m2);
+    return (cy + cz * g.m1) * g.m0;
+}
+
 // a mod M for a in (-M, 2M).
 __device__ __forceinline__ int wrap1(int a, int M) { return a < 0 ? a + M : (a >= M ? a - M : a); }
 
@@ -85,27 +109,6 @@ __device__ __forceinline__ unsigned rows_hit(int s, int r0, int M) {
         if (wrap1(r0 + b - s, M) < SLAB_MG) m |= 1u << b;
     return m;
 }
-
-// One window of listed particles and their separable weights.
-template <typename T, int BY, int BZ, int H>
-struct SlabWin {
-    static constexpr int NRP = BY * BZ;
-    int s[SLAB_CAP];          // sorted particle index
-    int key[SLAB_CAP];        // first x point of the stencil, in [0, Mx)
-    int sy[SLAB_CAP], sz[SLAB_CAP];
-    unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15)
-    T y0[SLAB_CAP], y1[SLAB_CAP], y2[SLAB_CAP];
-    T f[3][SLAB_CAP];
-    // rows padded by one element: lanes reading different entries at the same
-    // stencil point or slab row then fall into different banks
-    T gx[SLAB_CAP][SLAB_MG + 1], r2x[SLAB_CAP][SLAB_MG + 1];
-    T gyz[SLAB_CAP][NRP + 1], r2yz[SLAB_CAP][NRP + 1];
-    unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry)
-    int first[2 * H + 1];     // first sorted entry with key >= v
-    int pair_start[SLAB_PAIRMAX + 1];
-    int pair_sb[SLAB_PAIRMAX];
-    int scan[32];
-};
 
 // Block-wide exclusive scan of one int per thread (blockDim.x <= 1024).
 __device__ __forceinline__ int block_scan(int v, int* sm, int& total) {
@@ -147,172 +150,41 @@ __device__ __forceinline__ void slab_anchor(const StencilParams<T>& p, const vec
     m = (my && mz) ? (my | (mz << 8)) : 0u;
 }
 
-template <typename T, int BY, int BZ, int H>
-__device__ __forceinline__ void slab_put(SlabWin<T, BY, BZ, H>& W, int i, int s, const vec4<T>& y, int sx,
-                                         int sy, int sz, unsigned m) {
-    W.s[i] = s;
-    W.key[i] = wrap1(sx, 2 * H);
-    W.sy[i] = sy;
-    W.sz[i] = sz;
-    W.msk[i] = m;
-    W.y0[i] = y.x;
-    W.y1[i] = y.y;
-    W.y2[i] = y.z;
+// Gaussian factor and squared offset of stencil point g along one axis, with
+// the reference's x = g h - Y (src/stencil.jl:80-112).
+template <typename T>
+__device__ __forceinline__ void axis_weight(const StencilParams<T>& p, int g, T y, T& gw, T& r2) {
+    const T x = sub_rn(mul_rn((T)g, p.h), y);
+    r2 = mul_rn(x, x);
+    gw = p.inv_norm * exp_t(-r2 * p.inv_2S2);
 }
 
-// Separable weights of window entry i (one thread per entry), with the
-// reference's x = g h - Y for the unwrapped stencil point g. Row pairs the
-// particle does not reach keep weight 0 and are skipped by the mask.
-template <typename T, int BY, int BZ, int H>
-__device__ __forceinline__ void slab_entry_weights(const StencilParams<T>& p, SlabWin<T, BY, BZ, H>& W,
-                                                   int i, int y0r, int z0r) {
-    const int gx0 = (int)rint_t(mul_rn(W.y0[i], p.inv_h)) - SLAB_MG / 2;
-#pragma unroll
-    for (int e = 0; e < SLAB_MG; ++e) {
-        const T x = sub_rn(mul_rn((T)(gx0 + e), p.h), W.y0[i]);
-        const T x2 = mul_rn(x, x);
-        W.gx[i][e] = p.inv_norm * exp_t(-x2 * p.inv_2S2);
-        W.r2x[i][e] = x2;
-    }
-    const unsigned m = W.msk[i];
+// Per slab row r = d * BY + b: gy gz and r2y + r2z of a particle (zero for
+// rows the particle does not reach; the mask skips those).
+template <typename T, int BY, int BZ>
+__device__ __forceinline__ void row_weights(const StencilParams<T>& p, const vec4<T>& y, int sy, int sz,
+                                            unsigned m, int y0r, int z0r, T (&gyz)[BY * BZ],
+                                            T (&r2yz)[BY * BZ]) {
     T gy[BY], r2y[BY], gz[BZ], r2z[BZ];
 #pragma unroll
     for (int b = 0; b < BY; ++b) {
         gy[b] = T(0);
         r2y[b] = T(0);
-        if ((m >> b) & 1u) {
-            const int g = W.sy[i] + wrap1(y0r + b - W.sy[i], p.My);
-            const T x = sub_rn(mul_rn((T)g, p.h), W.y1[i]);
-            r2y[b] = mul_rn(x, x);
-            gy[b] = p.inv_norm * exp_t(-r2y[b] * p.inv_2S2);
-        }
+        if ((m >> b) & 1u) axis_weight(p, sy + wrap1(y0r + b - sy, p.My), y.y, gy[b], r2y[b]);
     }
 #pragma unroll
     for (int d = 0; d < BZ; ++d) {
         gz[d] = T(0);
         r2z[d] = T(0);
-        if ((m >> (8 + d)) & 1u) {
-            const int g = W.sz[i] + wrap1(z0r + d - W.sz[i], p.Mz);
-            const T x = sub_rn(mul_rn((T)g, p.h), W.y2[i]);
-            r2z[d] = mul_rn(x, x);
-            gz[d] = p.inv_norm * exp_t(-r2z[d] * p.inv_2S2);
-        }
+        if ((m >> (8 + d)) & 1u) axis_weight(p, sz + wrap1(z0r + d - sz, p.Mz), y.z, gz[d], r2z[d]);
     }
 #pragma unroll
     for (int d = 0; d < BZ; ++d)
 #pragma unroll
         for (int b = 0; b < BY; ++b) {
-            W.gyz[i][d * BY + b] = gy[b] * gz[d];
-            W.r2yz[i][d * BY + b] = r2y[b] + r2z[d];
+            gyz[d * BY + b] = gy[b] * gz[d];
+            r2yz[d * BY + b] = r2y[b] + r2z[d];
         }
-}
-
-// Scan the candidates of a slab (particles of the cell rows in range, in
-// sorted order) and hand the touching ones to `process(count)` in windows of
-// at most SLAB_CAP entries, in candidate order. Stores the full list in
-// glist (capacity g.lcap) and its length in *gcount (-1 when it did not fit).
-// All threads of the block must call this.
-template <typename T, int BY, int BZ, int H, bool WANT_F, typename Process>
-__device__ __forceinline__ void slab_scan(const vec4<T>* __restrict__ Ys, const vec4<T>* __restrict__ Fs,
-                                         const int32_t* __restrict__ off, const StencilParams<T>& p,
-                                         const SlabGeom& g, int y0r, int z0r, SlabWin<T, BY, BZ, H>& W,
-                                         int* __restrict__ glist, int* __restrict__ gcount,
-                                         Process&& process) {
-    constexpr int half = SLAB_MG / 2;
-    int cy_lo, ny, cz_lo, nz;
-    cell_span(y0r - SLAB_MG + 1 + half, y0r + BY - 1 + half, g.h, g.cs1, g.m1, cy_lo, ny);
-    cell_span(z0r - SLAB_MG + 1 + half, z0r + BZ - 1 + half, g.h, g.cs2, g.m2, cz_lo, nz);
-    const int npairs = ny * nz;   // <= SLAB_PAIRMAX (checked on the host)
-    int carry = 0;
-    for (int base = 0; base < npairs; base += blockDim.x) {
-        const int pi = base + threadIdx.x;
-        int len = 0;
-        if (pi < npairs) {
-            const int cy = imod(cy_lo + pi % ny, g.m1);
-            const int cz = imod(cz_lo + pi / ny, g.m2);
-            const int c0 = (cy + cz * g.m1) * g.m0;
-            const int sb = off[c0];
-            len = off[c0 + g.m0] - sb;
-            W.pair_sb[pi] = sb;
-        }
-        int tot;
-        const int pre = block_scan(len, W.scan, tot);
-        if (pi < npairs) W.pair_start[pi] = carry + pre;
-        carry += tot;
-    }
-    if (threadIdx.x == 0) W.pair_start[npairs] = carry;
-    __syncthreads();
-    const int ncand = carry;
-    int count = 0, total = 0;
-    // chunks of SLAB_CAP candidates, so one chunk always fits an emptied window
-    for (int c0 = 0; c0 < ncand; c0 += SLAB_CAP) {
-        const int c = c0 + threadIdx.x;
-        unsigned m = 0;
-        int s = 0, sx = 0, sy = 0, sz = 0;
-        vec4<T> y{};
-        if (threadIdx.x < SLAB_CAP && c < ncand) {
-            int lo = 0, hi = npairs - 1;   // last cell row with pair_start <= c
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (W.pair_start[mid] <= c) lo = mid;
-                else hi = mid - 1;
-            }
-            s = W.pair_sb[lo] + (c - W.pair_start[lo]);
-            y = Ys[s];
-            slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
-        }
-        int tot;
-        const int pre = block_scan(m ? 1 : 0, W.scan, tot);
-        if (count + tot > SLAB_CAP) {   // block-uniform
-            process(count);
-            __syncthreads();
-            count = 0;
-        }
-        if (m) {
-            const int i = count + pre;
-            slab_put(W, i, s, y, sx, sy, sz, m);
-            if (WANT_F) {
-                const vec4<T> f = Fs[s];
-                W.f[0][i] = f.x; W.f[1][i] = f.y; W.f[2][i] = f.z;
-            }
-            if (glist && total + pre < g.lcap) glist[total + pre] = s;
-        }
-        count += tot;
-        total += tot;
-        __syncthreads();
-    }
-    if (count > 0) process(count);
-    if (gcount && threadIdx.x == 0) *gcount = total <= g.lcap ? total : -1;
-    __syncthreads();
-}
-
-// Replay a stored slab list in windows of SLAB_CAP entries (the list holds
-// only particles that touch the slab, in candidate order).
-template <typename T, int BY, int BZ, int H, bool WANT_F, typename Process>
-__device__ __forceinline__ void slab_replay(const vec4<T>* __restrict__ Ys, const vec4<T>* __restrict__ Fs,
-                                           const StencilParams<T>& p, int y0r, int z0r,
-                                           SlabWin<T, BY, BZ, H>& W, const int* __restrict__ glist, int total,
-                                           Process&& process) {
-    for (int w0 = 0; w0 < total; w0 += SLAB_CAP) {
-        const int n = min(SLAB_CAP, total - w0);
-        if ((int)threadIdx.x < n) {
-            const int s = glist[w0 + threadIdx.x];
-            const vec4<T> y = Ys[s];
-            int sx, sy, sz;
-            unsigned m;
-            slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
-            slab_put(W, (int)threadIdx.x, s, y, sx, sy, sz, m);
-            if (WANT_F) {
-                const vec4<T> f = Fs[s];
-                W.f[0][threadIdx.x] = f.x;
-                W.f[1][threadIdx.x] = f.y;
-                W.f[2][threadIdx.x] = f.z;
-            }
-        }
-        __syncthreads();
-        process(n);
-        __syncthreads();
-    }
 }
 
 // Per-slab particle lists, one warp per slab: the candidates (particles of
@@ -323,22 +195,16 @@ __device__ __forceinline__ void slab_replay(const vec4<T>* __restrict__ Ys, cons
 template <typename T, int BY, int BZ>
 __global__ void k_slab_lists(const vec4<T>* __restrict__ Ys, const int32_t* __restrict__ off,
                              StencilParams<T> p, SlabGeom g, int* __restrict__ lists, int* __restrict__ counts) {
-    constexpr int half = SLAB_MG / 2;
     const int lane = threadIdx.x & 31;
     const int slab = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (slab >= g.nty * g.ntz) return;   // whole warps leave together
-    const int ty = slab % g.nty, tz = slab / g.nty;
-    const int y0r = ty * BY, z0r = tz * BZ;
-    int cy_lo, ny, cz_lo, nz;
-    cell_span(y0r - SLAB_MG + 1 + half, y0r + BY - 1 + half, g.h, g.cs1, g.m1, cy_lo, ny);
-    cell_span(z0r - SLAB_MG + 1 + half, z0r + BZ - 1 + half, g.h, g.cs2, g.m2, cz_lo, nz);
+    const int y0r = (slab % g.nty) * BY, z0r = (slab / g.nty) * BZ;
+    const SlabRows rows = slab_rows<BY, BZ>(g, y0r, z0r);
     int* out = lists + (int64_t)slab * g.lcap;
     const unsigned lt = (1u << lane) - 1u;
     int total = 0;
-    for (int pi = 0; pi < ny * nz; ++pi) {
-        const int cy = imod(cy_lo + pi % ny, g.m1);
-        const int cz = imod(cz_lo + pi / ny, g.m2);
-        const int c0 = (cy + cz * g.m1) * g.m0;
+    for (int pi = 0; pi < rows.ny * rows.nz; ++pi) {
+        const int c0 = slab_row_cell(g, rows, pi);
         const int sb = off[c0], se = off[c0 + g.m0];
         for (int b = sb; b < se; b += 32) {
             const int s = b + lane;
@@ -358,6 +224,43 @@ __global__ void k_slab_lists(const vec4<T>* __restrict__ Ys, const int32_t* __re
     if (lane == 0) counts[slab] = total <= g.lcap ? total : -1;
 }
 
+// One window of the spread: per entry the first x point of its stencil, the
+// slab rows it reaches, its x position, force, and per-row weight parts.
+template <typename T, int BY, int BZ, int H>
+struct SpreadWin {
+    static constexpr int NRP = BY * BZ;
+    int key[SLAB_CAP];        // first x point of the stencil, in [0, Mx)
+    unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15)
+    T y0[SLAB_CAP];
+    T f[3][SLAB_CAP];
+    // rows padded by one element: lanes reading different entries at the same
+    // slab row then fall into different banks
+    T gyz[SLAB_CAP][NRP + 1], r2yz[SLAB_CAP][NRP + 1];
+    unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry)
+    int first[2 * H + 1];     // first sorted entry with key >= v
+    int scan[32];
+};
+
+template <typename T, int BY, int BZ, int H>
+__device__ __forceinline__ void spread_put(const StencilParams<T>& p, SpreadWin<T, BY, BZ, H>& W, int i,
+                                           const vec4<T>& y, const vec4<T>& f, int sx, int sy, int sz,
+                                           unsigned m, int y0r, int z0r) {
+    constexpr int NRP = BY * BZ;
+    W.key[i] = wrap1(sx, 2 * H);
+    W.msk[i] = m;
+    W.y0[i] = y.x;
+    W.f[0][i] = f.x;
+    W.f[1][i] = f.y;
+    W.f[2][i] = f.z;
+    T gyz[NRP], r2yz[NRP];
+    row_weights<T, BY, BZ>(p, y, sy, sz, m, y0r, z0r, gyz, r2yz);
+#pragma unroll
+    for (int r = 0; r < NRP; ++r) {
+        W.gyz[i][r] = gyz[r];
+        W.r2yz[i][r] = r2yz[r];
+    }
+}
+
 // ---- spread into a slab, then x-r2c straight into the spectrum -----------
 template <typename T, int H, int BY, int BZ>
 __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__ Ys,
@@ -371,91 +274,136 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
     constexpr int Mx = 2 * H, P = slab_pitch(Mx), NRP = BY * BZ, ROWS = 3 * NRP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
-    cplx<T>* tw = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
-    cplx<T>* dummy = tw + Mx;   // exchange of the idle lanes of a partial FFT round
-    SlabWin<T, BY, BZ, H>& W = *reinterpret_cast<SlabWin<T, BY, BZ, H>*>(dummy + padded_len(H));
+    SpreadWin<T, BY, BZ, H>& W = *reinterpret_cast<SpreadWin<T, BY, BZ, H>*>(acc + ROWS * P);
+    // exchange line of idle FFT lanes: the window is dead by then
+    cplx<T>* dummy = reinterpret_cast<cplx<T>*>(&W);
+    const cplx<T>* tw = twx;   // twiddles are read through L1
     const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
     for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
-    load_table(tw, twx, Mx);
     __syncthreads();
+    // Window entries [0, count) are in W; all threads call this after a barrier.
     auto process = [&](int count) {
-            __syncthreads();
-            // sort the window by first x point: each entry's rank is the
-            // number of entries with a smaller (key, index) pair
-            for (int i = threadIdx.x; i < SLAB_CAP; i += blockDim.x) {
-                if (i < count) {
-                    slab_entry_weights(p, W, i, y0r, z0r);
-                    const unsigned me = ((unsigned)W.key[i] << 7) | (unsigned)i;
-                    int rank = 0;
-                    for (int k = 0; k < count; ++k) rank += (((unsigned)W.key[k] << 7) | (unsigned)k) < me;
-                    W.sk[rank] = me;
+        // order the window by first x point: each entry's rank is the number
+        // of entries with a smaller (key, index) pair
+        for (int i = threadIdx.x; i < SLAB_CAP; i += blockDim.x) {
+            if (i < count) {
+                const unsigned me = ((unsigned)W.key[i] << 7) | (unsigned)i;
+                int rank = 0;
+                for (int k = 0; k < count; ++k) rank += (((unsigned)W.key[k] << 7) | (unsigned)k) < me;
+                W.sk[rank] = me;
+            } else {
+                W.sk[i] = 0xffffffffu;
+            }
+        }
+        __syncthreads();
+        for (int v = threadIdx.x; v <= Mx; v += blockDim.x) {
+            int lo = 0, hi = SLAB_CAP;   // first sorted entry with key >= v
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if ((int)(W.sk[mid] >> 7) < v) lo = mid + 1;
+                else hi = mid;
+            }
+            W.first[v] = lo;
+        }
+        __syncthreads();
+        // gather: each thread owns grid points x of all slab rows
+        for (int x = threadIdx.x; x < Mx; x += blockDim.x) {
+            T a[3][NRP];
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+                for (int r = 0; r < NRP; ++r) a[c][r] = T(0);
+            const int lo1 = x - SLAB_MG + 1;
+            // entries whose stencil starts in [lo1, x] (periodic in x)
+            for (int part = 0; part < 2; ++part) {
+                int kb, ke;
+                if (part == 0) {
+                    kb = W.first[lo1 >= 0 ? lo1 : 0];
+                    ke = W.first[x + 1];
                 } else {
-                    W.sk[i] = 0xffffffffu;
+                    if (lo1 >= 0) break;
+                    kb = W.first[Mx + lo1];
+                    ke = W.first[Mx];
+                }
+                for (int kk = kb; kk < ke; ++kk) {
+                    const unsigned v = W.sk[kk];
+                    const int i = (int)(v & 127u);
+                    int e = x - (int)(v >> 7);
+                    if (e < 0) e += Mx;
+                    const T y0 = W.y0[i];
+                    const int gx0 = (int)rint_t(mul_rn(y0, p.inv_h)) - SLAB_MG / 2;
+                    T gxe, r2xe;
+                    axis_weight(p, gx0 + e, y0, gxe, r2xe);
+                    const unsigned m = W.msk[i];
+                    const T f0 = W.f[0][i], f1 = W.f[1][i], f2 = W.f[2][i];
+#pragma unroll
+                    for (int d = 0; d < BZ; ++d)
+#pragma unroll
+                        for (int b = 0; b < BY; ++b) {
+                            if (!((m >> b) & (m >> (8 + d)) & 1u)) continue;
+                            const int r = d * BY + b;
+                            const T wgt = (p.a0 + p.a2 * (r2xe + W.r2yz[i][r])) * gxe * W.gyz[i][r];
+                            a[0][r] += wgt * f0;
+                            a[1][r] += wgt * f1;
+                            a[2][r] += wgt * f2;
+                        }
                 }
             }
-            __syncthreads();
-            for (int v = threadIdx.x; v <= Mx; v += blockDim.x) {
-                int lo = 0, hi = SLAB_CAP;   // first sorted entry with key >= v
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if ((int)(W.sk[mid] >> 7) < v) lo = mid + 1;
-                    else hi = mid;
-                }
-                W.first[v] = lo;
-            }
-            __syncthreads();
-            // gather: each thread owns grid points x of all slab rows
-            for (int x = threadIdx.x; x < Mx; x += blockDim.x) {
-                T a[3][NRP];
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
+            for (int c = 0; c < 3; ++c)
 #pragma unroll
-                    for (int r = 0; r < NRP; ++r) a[c][r] = T(0);
-                const int lo1 = x - SLAB_MG + 1;
-                // entries whose stencil starts in [lo1, x] (periodic in x)
-                for (int part = 0; part < 2; ++part) {
-                    int kb, ke;
-                    if (part == 0) {
-                        kb = W.first[lo1 >= 0 ? lo1 : 0];
-                        ke = W.first[x + 1];
-                    } else {
-                        if (lo1 >= 0) break;
-                        kb = W.first[Mx + lo1];
-                        ke = W.first[Mx];
-                    }
-                    for (int kk = kb; kk < ke; ++kk) {
-                        const unsigned v = W.sk[kk];
-                        const int i = (int)(v & 127u);
-                        int e = x - (int)(v >> 7);
-                        if (e < 0) e += Mx;
-                        const T gxe = W.gx[i][e], r2xe = W.r2x[i][e];
-                        const unsigned m = W.msk[i];
-                        const T f0 = W.f[0][i], f1 = W.f[1][i], f2 = W.f[2][i];
-#pragma unroll
-                        for (int d = 0; d < BZ; ++d)
-#pragma unroll
-                            for (int b = 0; b < BY; ++b) {
-                                if (!((m >> b) & (m >> (8 + d)) & 1u)) continue;
-                                const int r = d * BY + b;
-                                const T wgt = (p.a0 + p.a2 * (r2xe + W.r2yz[i][r])) * gxe * W.gyz[i][r];
-                                a[0][r] += wgt * f0;
-                                a[1][r] += wgt * f1;
-                                a[2][r] += wgt * f2;
-                            }
-                    }
-                }
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-#pragma unroll
-                    for (int r = 0; r < NRP; ++r) acc[(c * NRP + r) * P + x] += a[c][r];
-            }
-        };
+                for (int r = 0; r < NRP; ++r) acc[(c * NRP + r) * P + x] += a[c][r];
+        }
+    };
     const int stored = counts[cta];
     if (stored >= 0) {
-        slab_replay<T, BY, BZ, H, true>(Ys, Fs, p, y0r, z0r, W, lists + (int64_t)cta * g.lcap, stored, process);
+        const int* glist = lists + (int64_t)cta * g.lcap;
+        for (int w0 = 0; w0 < stored; w0 += SLAB_CAP) {
+            const int n = min(SLAB_CAP, stored - w0);
+            if ((int)threadIdx.x < n) {
+                const int s = glist[w0 + threadIdx.x];
+                const vec4<T> y = Ys[s];
+                int sx, sy, sz;
+                unsigned m;
+                slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
+                spread_put(p, W, (int)threadIdx.x, y, Fs[s], sx, sy, sz, m, y0r, z0r);
+            }
+            __syncthreads();
+            process(n);
+            __syncthreads();
+        }
     } else {
-        slab_scan<T, BY, BZ, H, true>(Ys, Fs, off, p, g, y0r, z0r, W, nullptr, nullptr, process);
+        // the list overflowed: scan the candidates in chunks of SLAB_CAP and
+        // compact the touching ones into windows, in candidate order
+        const SlabRows rows = slab_rows<BY, BZ>(g, y0r, z0r);
+        int count = 0;
+        for (int pi = 0; pi < rows.ny * rows.nz; ++pi) {
+            const int c0 = slab_row_cell(g, rows, pi);
+            const int sb = off[c0], se = off[c0 + g.m0];
+            for (int b = sb; b < se; b += SLAB_CAP) {
+                const int s = b + (int)threadIdx.x;
+                unsigned m = 0;
+                int sx = 0, sy = 0, sz = 0;
+                vec4<T> y{};
+                if ((int)threadIdx.x < SLAB_CAP && s < se) {
+                    y = Ys[s];
+                    slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
+                }
+                int tot;
+                const int pre = block_scan(m ? 1 : 0, W.scan, tot);
+                if (count + tot > SLAB_CAP) {   // block-uniform
+                    process(count);
+                    __syncthreads();
+                    count = 0;
+                }
+                if (m) spread_put(p, W, count + pre, y, Fs[s], sx, sy, sz, m, y0r, z0r);
+                count += tot;
+                __syncthreads();
+            }
+        }
+        if (count > 0) process(count);
+        __syncthreads();
     }
     // x r2c of every slab row (H/8 threads per row), output straight to spec.
     // A row that fits one warp is transformed with warp-level synchronisation
@@ -465,7 +413,6 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
     constexpr bool WARP = TPL <= 32;
     const int lines_per_round = blockDim.x / TPL;
     const int lr = threadIdx.x / TPL, j = threadIdx.x - lr * TPL;
-    __syncthreads();
     for (int r0 = 0; r0 < ROWS; r0 += lines_per_round) {
         const int r = r0 + lr;
         const bool active = r < ROWS && lr < lines_per_round;
@@ -516,13 +463,10 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
     constexpr int Mx = 2 * H, P = slab_pitch(Mx), NRP = BY * BZ, ROWS = 3 * NRP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
-    cplx<T>* tw = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
-    cplx<T>* dummy = tw + Mx;
-    SlabWin<T, BY, BZ, H>& W = *reinterpret_cast<SlabWin<T, BY, BZ, H>*>(dummy + padded_len(H));
+    cplx<T>* dummy = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
+    const cplx<T>* tw = twx;   // twiddles are read through L1
     const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
-    load_table(tw, twx, Mx);
-    __syncthreads();
     constexpr int TPL = H / 8, Q = H / 8;
     constexpr bool WARP = TPL <= 32;
     const int lines_per_round = blockDim.x / TPL;
@@ -558,45 +502,53 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
         if (WARP) __syncwarp(); else __syncthreads();
     }
     __syncthreads();
-    auto gather = [&](int count) {
-        for (int i = threadIdx.x; i < count; i += blockDim.x) {
-            slab_entry_weights(p, W, i, y0r, z0r);
-            const unsigned m = W.msk[i];
-            const int x0 = W.key[i];
-            T v0 = 0, v1 = 0, v2 = 0;
+    // one thread per particle: weights in registers, gather over the slab rows
+    auto gather = [&](int s) {
+        const vec4<T> y = Ys[s];
+        int sx, sy, sz;
+        unsigned m;
+        slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
+        if (!m) return;
+        T gyz[NRP], r2yz[NRP], gx[SLAB_MG], r2x[SLAB_MG];
+        row_weights<T, BY, BZ>(p, y, sy, sz, m, y0r, z0r, gyz, r2yz);
 #pragma unroll
-            for (int d = 0; d < BZ; ++d)
+        for (int e = 0; e < SLAB_MG; ++e) axis_weight(p, sx + e, y.x, gx[e], r2x[e]);
+        const int x0 = wrap1(sx, Mx);
+        T v0 = 0, v1 = 0, v2 = 0;
 #pragma unroll
-                for (int b = 0; b < BY; ++b) {
-                    if (!((m >> b) & (m >> (8 + d)) & 1u)) continue;
-                    const int r = d * BY + b;
-                    const T r2yz = W.r2yz[i][r], gyz = W.gyz[i][r];
-                    const T* row = acc + r * P;
+        for (int d = 0; d < BZ; ++d)
 #pragma unroll
-                    for (int e = 0; e < SLAB_MG; ++e) {
-                        int x = x0 + e;
-                        if (x >= Mx) x -= Mx;
-                        const T wgt = (p.a0 + p.a2 * (W.r2x[i][e] + r2yz)) * W.gx[i][e] * gyz;
-                        v0 += wgt * row[x];
-                        v1 += wgt * row[NRP * P + x];
-                        v2 += wgt * row[2 * NRP * P + x];
-                    }
+            for (int b = 0; b < BY; ++b) {
+                if (!((m >> b) & (m >> (8 + d)) & 1u)) continue;
+                const int r = d * BY + b;
+                const T* row = acc + r * P;
+#pragma unroll
+                for (int e = 0; e < SLAB_MG; ++e) {
+                    int x = x0 + e;
+                    if (x >= Mx) x -= Mx;
+                    const T wgt = (p.a0 + p.a2 * (r2x[e] + r2yz[r])) * gx[e] * gyz[r];
+                    v0 += wgt * row[x];
+                    v1 += wgt * row[NRP * P + x];
+                    v2 += wgt * row[2 * NRP * P + x];
                 }
-            T* vs = Vs + 3 * (int64_t)W.s[i];
-            atomicAdd(vs, v0);
-            atomicAdd(vs + 1, v1);
-            atomicAdd(vs + 2, v2);
-        }
+            }
+        T* vs = Vs + 3 * (int64_t)s;
+        atomicAdd(vs, v0);
+        atomicAdd(vs + 1, v1);
+        atomicAdd(vs + 2, v2);
     };
     const int stored = counts[cta];
     if (stored >= 0) {
-        slab_replay<T, BY, BZ, H, false>(Ys, nullptr, p, y0r, z0r, W, lists + (int64_t)cta * g.lcap, stored, gather);
+        const int* glist = lists + (int64_t)cta * g.lcap;
+        for (int t = threadIdx.x; t < stored; t += blockDim.x) gather(glist[t]);
     } else {
-        slab_scan<T, BY, BZ, H, false>(Ys, nullptr, off, p, g, y0r, z0r, W, nullptr, nullptr,
-                                      [&](int count) {
-                                          __syncthreads();
-                                          gather(count);
-                                      });
+        // the list overflowed: every candidate of the slab's cell rows
+        const SlabRows rows = slab_rows<BY, BZ>(g, y0r, z0r);
+        for (int pi = 0; pi < rows.ny * rows.nz; ++pi) {
+            const int c0 = slab_row_cell(g, rows, pi);
+            const int se = off[c0 + g.m0];
+            for (int s = off[c0] + (int)threadIdx.x; s < se; s += blockDim.x) gather(s);
+        }
     }
 }
 
@@ -616,7 +568,8 @@ struct SlabKernels {
     InterpSlabKernel<T> interp = nullptr;
     ListsKernel<T> lists = nullptr;
     int BY = 0, BZ = 0;
-    size_t smem = 0;
+    size_t smem = 0;          // spread
+    size_t smem_interp = 0;   // interpolation
 };
 
 template <typename T, int H>
@@ -628,8 +581,10 @@ SlabKernels<T> slab_kernels_for() {
     k.lists = k_slab_lists<T, BY, BZ>;
     k.BY = BY;
     k.BZ = BZ;
-    k.smem = (size_t)3 * BY * BZ * slab_pitch(2 * H) * sizeof(T) +
-             (size_t)(2 * H + padded_len(H)) * sizeof(cplx<T>) + sizeof(SlabWin<T, BY, BZ, H>);
+    const size_t slab_bytes = (size_t)3 * BY * BZ * slab_pitch(2 * H) * sizeof(T);
+    const size_t line_bytes = (size_t)padded_len(H) * sizeof(cplx<T>);
+    k.smem = slab_bytes + std::max(sizeof(SpreadWin<T, BY, BZ, H>), line_bytes);
+    k.smem_interp = slab_bytes + line_bytes;
     return k;
 }
 
