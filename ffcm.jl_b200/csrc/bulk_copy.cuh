@@ -1,0 +1,55 @@
+// Bulk asynchronous copies from global to shared memory (the TMA's untiled
+// form, cp.async.bulk) with an mbarrier for completion. Each block fills only
+// its own shared memory from this GPU's memory. Addresses and sizes must be
+// multiples of 16 bytes.
+#pragma once
+
+#include "common.cuh"
+
+namespace ffcm {
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    // make the initialised barrier visible to the copy engine
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Arrive once and announce `bytes` of copies that will complete on `bar`.
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for phase `parity` of `bar` with an iteration limit; false if it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity, int max_iter) {
+    for (int it = 0; it < max_iter; ++it)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// global -> shared, completing `bytes` of transactions on `bar`.
+__device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_global, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst_smem)),
+        "l"(src_global), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+}  // namespace ffcm

@@ -10,6 +10,7 @@ namespace ffcm {
 enum : int {
     DEVERR_NONFINITE_POSITION = 1,
     DEVERR_INDEX_RANGE = 2,
+    DEVERR_COPY_TIMEOUT = 4,   // a bounded wait for a bulk copy gave up
 };
 
 template <typename T>

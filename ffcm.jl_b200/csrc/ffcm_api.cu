@@ -790,7 +790,7 @@ struct Engine final : EngineBase {
         dim3 g(sg.nty, sg.ntz, 1);
         return launch(h, sk.interp, g, 256, sk.smem_interp, s, (const vec4<T>*)Ys, (const int32_t*)off,
                       (const cplx<T>*)spec, hxp, partial, sp, sg, (const cplx<T>*)twx,
-                      (const int*)slab_lists, (const int*)slab_counts);
+                      (const int*)slab_lists, (const int*)slab_counts, h->d_err);
     }
 
     int mobility_rest(void* V, cudaStream_t s) override { return solve(V, s, false); }
@@ -1026,6 +1026,8 @@ int finish(ffcm_handle* h, cudaStream_t s) {
         CUDA_TRY(cudaStreamSynchronize(s));
         if (e & DEVERR_NONFINITE_POSITION)
             return fail(FFCM_ERR_ARGUMENT, "non-finite particle position (InexactError in the reference)");
+        if (e & DEVERR_COPY_TIMEOUT)
+            return fail(FFCM_ERR_TIMEOUT, "a bounded device-side wait for a bulk copy gave up");
         return fail(FFCM_ERR_CUDA, "device-side error flag " + std::to_string(e));
     }
     return FFCM_OK;

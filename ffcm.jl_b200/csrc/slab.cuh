@@ -27,6 +27,7 @@
 // itself (same candidates, same order).
 #pragma once
 
+#include "bulk_copy.cuh"
 #include "common.cuh"
 #include "fft_pow2.cuh"
 #include "spread_interp.cuh"
@@ -452,6 +453,13 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
 // ---- x-c2r of a slab into shared memory, then gather partial velocities ----
 // Each slab adds its partial sums into Vs[3 s + c] (sorted order, zeroed
 // beforehand); the correction kernel finishes V[:, perm[s]] = h^3 Vs[s] + dv.
+// Bytes of a spectrum row copied into a slab row: H + 1 complex values,
+// rounded up to 16 bytes (the spectrum pitch and the slab pitch hold them).
+template <typename T, int H>
+__host__ __device__ constexpr unsigned slab_row_copy_bytes() {
+    return (unsigned)(((H + 1) * sizeof(cplx<T>) + 15) / 16 * 16);
+}
+
 template <typename T, int H, int BY, int BZ>
 __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__ Ys,
                                                      const int32_t* __restrict__ off,
@@ -459,14 +467,38 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
                                                      T* __restrict__ Vs, StencilParams<T> p,
                                                      SlabGeom g, const cplx<T>* __restrict__ twx,
                                                      const int* __restrict__ lists,
-                                                     const int* __restrict__ counts) {
+                                                     const int* __restrict__ counts, int* __restrict__ err) {
     constexpr int Mx = 2 * H, P = slab_pitch(Mx), NRP = BY * BZ, ROWS = 3 * NRP;
+    constexpr unsigned RB = slab_row_copy_bytes<T, H>();
+    static_assert(RB <= P * sizeof(T), "a spectrum row must fit a slab row");
+    static_assert((P * sizeof(T)) % 16 == 0, "slab rows must start on 16-byte boundaries");
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
     T* acc = reinterpret_cast<T*>(smem_raw);
     cplx<T>* dummy = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
     const cplx<T>* tw = twx;   // twiddles are read through L1
     const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
+    // all of the slab's spectrum rows arrive in one batch of bulk copies
+    // (row starts are 16-byte aligned: the spectrum pitch is a multiple of
+    // 128 bytes)
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_arrive_expect(&bar, ROWS * RB);
+        for (int r = 0; r < ROWS; ++r) {
+            const int c = r / NRP, bd = r % NRP;
+            const cplx<T>* src = spec + (((int64_t)c * p.Mz + z0r + bd / BY) * p.My + y0r + bd % BY) * hxp;
+            bulk_load(acc + r * P, src, RB, &bar);
+        }
+    }
+    __syncthreads();
+    if (!mbar_wait_bounded(&bar, 0, 1 << 22)) {
+        // the copies did not finish: report, give them one more bounded
+        // chance to land in this block's shared memory, and leave
+        if (threadIdx.x == 0) atomicOr(err, DEVERR_COPY_TIMEOUT);
+        mbar_wait_bounded(&bar, 0, 1 << 22);
+        return;
+    }
     constexpr int TPL = H / 8, Q = H / 8;
     constexpr bool WARP = TPL <= 32;
     const int lines_per_round = blockDim.x / TPL;
@@ -474,9 +506,7 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
     for (int r0 = 0; r0 < ROWS; r0 += lines_per_round) {
         const int r = r0 + lr;
         const bool active = r < ROWS && lr < lines_per_round;
-        const int c = active ? r / NRP : 0, bd = active ? r % NRP : 0;
-        const int b = bd % BY, d = bd / BY;
-        const cplx<T>* src = spec + (((int64_t)c * p.Mz + z0r + d) * p.My + y0r + b) * hxp;
+        const cplx<T>* src = reinterpret_cast<const cplx<T>*>(acc + (active ? r : 0) * P);
         cplx<T> v[8];
 #pragma unroll
         for (int qq = 0; qq < 8; ++qq) {
@@ -560,7 +590,7 @@ template <typename T>
 using ListsKernel = void (*)(const vec4<T>*, const int32_t*, StencilParams<T>, SlabGeom, int*, int*);
 template <typename T>
 using InterpSlabKernel = void (*)(const vec4<T>*, const int32_t*, const cplx<T>*, int, T*,
-                                  StencilParams<T>, SlabGeom, const cplx<T>*, const int*, const int*);
+                                  StencilParams<T>, SlabGeom, const cplx<T>*, const int*, const int*, int*);
 
 template <typename T>
 struct SlabKernels {
