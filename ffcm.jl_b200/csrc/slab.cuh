@@ -236,7 +236,7 @@ struct SpreadWin {
     T f[3][SLAB_CAP];
     // rows padded by one element: lanes reading different entries at the same
     // slab row then fall into different banks
-    T gyz[SLAB_CAP][NRP + 1], r2yz[SLAB_CAP][NRP + 1];
+    T gyz[SLAB_CAP][NRP + 1], dyz[SLAB_CAP][NRP + 1];   // gy gz and gy gz (r2y + r2z)
     unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry)
     int first[2 * H + 1];     // first sorted entry with key >= v
     int scan[32];
@@ -258,7 +258,7 @@ __device__ __forceinline__ void spread_put(const StencilParams<T>& p, SpreadWin<
 #pragma unroll
     for (int r = 0; r < NRP; ++r) {
         W.gyz[i][r] = gyz[r];
-        W.r2yz[i][r] = r2yz[r];
+        W.dyz[i][r] = gyz[r] * r2yz[r];
     }
 }
 
@@ -336,6 +336,8 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
                     const int gx0 = (int)rint_t(mul_rn(y0, p.inv_h)) - SLAB_MG / 2;
                     T gxe, r2xe;
                     axis_weight(p, gx0 + e, y0, gxe, r2xe);
+                    // (a0 + a2 (r2x + r2yz)) gx gyz = [gx (a0 + a2 r2x)] gyz + [a2 gx] [gyz r2yz]
+                    const T wa = gxe * (p.a0 + p.a2 * r2xe), wc = p.a2 * gxe;
                     const unsigned m = W.msk[i];
                     const T f0 = W.f[0][i], f1 = W.f[1][i], f2 = W.f[2][i];
 #pragma unroll
@@ -344,7 +346,7 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
                         for (int b = 0; b < BY; ++b) {
                             if (!((m >> b) & (m >> (8 + d)) & 1u)) continue;
                             const int r = d * BY + b;
-                            const T wgt = (p.a0 + p.a2 * (r2xe + W.r2yz[i][r])) * gxe * W.gyz[i][r];
+                            const T wgt = wa * W.gyz[i][r] + wc * W.dyz[i][r];
                             a[0][r] += wgt * f0;
                             a[1][r] += wgt * f1;
                             a[2][r] += wgt * f2;
@@ -539,10 +541,18 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
         unsigned m;
         slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
         if (!m) return;
-        T gyz[NRP], r2yz[NRP], gx[SLAB_MG], r2x[SLAB_MG];
+        T gyz[NRP], r2yz[NRP], wa[SLAB_MG], wc[SLAB_MG];
         row_weights<T, BY, BZ>(p, y, sy, sz, m, y0r, z0r, gyz, r2yz);
 #pragma unroll
-        for (int e = 0; e < SLAB_MG; ++e) axis_weight(p, sx + e, y.x, gx[e], r2x[e]);
+        for (int r = 0; r < NRP; ++r) r2yz[r] *= gyz[r];   // now gy gz (r2y + r2z)
+        // (a0 + a2 (r2x + r2yz)) gx gyz = [gx (a0 + a2 r2x)] gyz + [a2 gx] [gyz r2yz]
+#pragma unroll
+        for (int e = 0; e < SLAB_MG; ++e) {
+            T gxe, r2xe;
+            axis_weight(p, sx + e, y.x, gxe, r2xe);
+            wa[e] = gxe * (p.a0 + p.a2 * r2xe);
+            wc[e] = p.a2 * gxe;
+        }
         const int x0 = wrap1(sx, Mx);
         T v0 = 0, v1 = 0, v2 = 0;
 #pragma unroll
@@ -556,7 +566,7 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
                 for (int e = 0; e < SLAB_MG; ++e) {
                     int x = x0 + e;
                     if (x >= Mx) x -= Mx;
-                    const T wgt = (p.a0 + p.a2 * (r2x[e] + r2yz[r])) * gx[e] * gyz[r];
+                    const T wgt = wa[e] * gyz[r] + wc[e] * r2yz[r];
                     v0 += wgt * row[x];
                     v1 += wgt * row[NRP * P + x];
                     v2 += wgt * row[2 * NRP * P + x];
