@@ -210,6 +210,9 @@ struct EngineBase {
     virtual int interp(void* V, cudaStream_t s) = 0;
     virtual int correct(void* V, cudaStream_t s) = 0;
     virtual int mobility_rest(void* V, cudaStream_t s) = 0;
+    // a further right-hand side on the positions of the last solve (the
+    // cell list and the slab particle lists are reused)
+    virtual int mobility_rest_same_positions(void* V, cudaStream_t s) = 0;
     virtual int gather_forces(const void* F, cudaStream_t s) = 0;
     virtual int forward_checkpoint(void* V, cudaStream_t s) = 0;
     virtual int adjoint(const void* lam, void* dY, void* dF, cudaStream_t s) = 0;
@@ -745,11 +748,12 @@ struct Engine final : EngineBase {
     // spectrum, y/z passes, then x-c2r fused with the interpolation.
     bool fused_available() const { return slab; }
 
-    int spread_to_spectrum(cudaStream_t s, const vec4<T>* force = nullptr) {
+    int spread_to_spectrum(cudaStream_t s, const vec4<T>* force = nullptr, bool build_lists = true) {
         StageScope sc(h, FFCM_STAGE_SPREAD, s);
         const int nslab = sg.nty * sg.ntz;
-        TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
-                   slab_lists, slab_counts));
+        if (build_lists)
+            TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
+                       slab_lists, slab_counts));
         dim3 g(sg.nty, sg.ntz, 1);
         return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys, force ? force : (const vec4<T>*)Fs,
                       (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, (const int*)slab_lists,
@@ -794,17 +798,18 @@ struct Engine final : EngineBase {
     }
 
     int mobility_rest(void* V, cudaStream_t s) override { return solve(V, s, false); }
+    int mobility_rest_same_positions(void* V, cudaStream_t s) override { return solve(V, s, false, false); }
 
     // keep_u: also leave the velocity grid u = L^-1 S F in gu (the adjoint's
     // only checkpoint); the unfused pipeline leaves it there anyway.
-    int solve(void* V, cudaStream_t s, bool keep_u) {
+    int solve(void* V, cudaStream_t s, bool keep_u, bool build_lists = true) {
         if (!slab) {
             TRY(spread(s));
             TRY(stokes(s));
             TRY(interp(V, s));
             return correct(V, s);
         }
-        TRY(spread_to_spectrum(s));
+        TRY(spread_to_spectrum(s, nullptr, build_lists));
         TRY(stokes_yz(s));
         if (keep_u) {
             StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
@@ -870,7 +875,7 @@ struct Engine final : EngineBase {
                        static_cast<const T*>(lam), Ls));
         }
         if (slab) {
-            TRY(spread_to_spectrum(s, Ls));
+            TRY(spread_to_spectrum(s, Ls, false));   // the checkpoint's lists
             TRY(stokes_yz(s));
             StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
             TRY(x_inverse(gpsi, s));
@@ -1656,7 +1661,7 @@ int batch_build_graph(ffcm_batch* b) {
         if (rc == FFCM_OK) rc = e->mobility_rest(Vr(0), s);
         for (int r = 1; r < b->nrhs && rc == FFCM_OK; ++r) {
             rc = e->gather_forces(Fr(r), s);
-            if (rc == FFCM_OK) rc = e->mobility_rest(Vr(r), s);
+            if (rc == FFCM_OK) rc = e->mobility_rest_same_positions(Vr(r), s);
         }
         if (rc == FFCM_OK && (cudaEventRecord(b->ev[1 + i], s) != cudaSuccess ||
                               cudaStreamWaitEvent(b->main, b->ev[1 + i], 0) != cudaSuccess))
