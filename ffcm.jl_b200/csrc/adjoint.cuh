@@ -162,12 +162,18 @@ __device__ __forceinline__ void correction_scalars_d(T r, const CorrConsts<T>& c
 // neighbour cells of the forward correction (same pair set):
 //   dF[:, perm[s]] += self lam_n + sum_m T(x) lam_m
 //   dY[:, perm[s]] += sum_m grad_x [lam_n . T(x) F_m + lam_m . T(x) F_n]
-template <typename T>
+template <typename T, int TPP>
 __global__ void k_correct_adjoint(int n_part, const vec4<T>* __restrict__ Ys, const vec4<T>* __restrict__ Fs,
                                   const vec4<T>* __restrict__ Ls, const int32_t* __restrict__ off,
                                   const int32_t* __restrict__ perm, T* __restrict__ dY, T* __restrict__ dF,
                                   CorrConsts<T> c, CorrGradConsts<T> cg) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_part; s += gridDim.x * blockDim.x) {
+    // TPP lanes per particle share its 27 neighbour cells (as in k_correct)
+    const int sub = threadIdx.x % TPP;
+    const unsigned group = ((1u << TPP) - 1u) << (lane_id() & ~(TPP - 1));
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n_part * TPP;
+         t += nthreads) {
+        const int s = (int)(t / TPP);
         const vec4<T> yn = Ys[s], fn = Fs[s], ln = Ls[s];
         int cx = (int)floor_t(mul_rn(yn.x, c.ic0));
         int cy = (int)floor_t(mul_rn(yn.y, c.ic1));
@@ -176,52 +182,64 @@ __global__ void k_correct_adjoint(int n_part, const vec4<T>* __restrict__ Ys, co
         cy = max(0, min(cy, c.m1 - 1));
         cz = max(0, min(cz, c.m2 - 1));
         T g0 = 0, g1 = 0, g2 = 0;
-        T v0 = c.self * ln.x, v1 = c.self * ln.y, v2 = c.self * ln.z;
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int nz = imod(cz + dz, c.m2);
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int ny = imod(cy + dy, c.m1);
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int nx = imod(cx + dx, c.m0);
-                    const int cn = nx + (ny + nz * c.m1) * c.m0;
-                    const int e = off[cn + 1];
-                    for (int s2 = off[cn]; s2 < e; ++s2) {
-                        if (s2 == s) continue;
-                        const vec4<T> ym = Ys[s2];
-                        const T x0 = min_image(sub_rn(yn.x, ym.x), c.L0);
-                        const T x1 = min_image(sub_rn(yn.y, ym.y), c.L1);
-                        const T x2 = min_image(sub_rn(yn.z, ym.z), c.L2);
-                        const T rr = add_rn(add_rn(mul_rn(x0, x0), mul_rn(x1, x1)), mul_rn(x2, x2));
-                        if (!(rr < c.Rc2)) continue;
-                        const T r = sqrt_t(rr);
-                        T A, B, dA, dB;
-                        correction_scalars_d(r, c, cg, A, B, dA, dB);
-                        const vec4<T> fm = Fs[s2], lm = Ls[s2];
-                        const T lnx = ln.x * x0 + ln.y * x1 + ln.z * x2;
-                        const T lmx = lm.x * x0 + lm.y * x1 + lm.z * x2;
-                        const T xfm = x0 * fm.x + x1 * fm.y + x2 * fm.z;
-                        const T xfn = x0 * fn.x + x1 * fn.y + x2 * fn.z;
-                        const T P = ln.x * fm.x + ln.y * fm.y + ln.z * fm.z + lm.x * fn.x + lm.y * fn.y +
-                                    lm.z * fn.z;
-                        const T radial = (dA * P + dB * (lnx * xfm + lmx * xfn)) / r;
-                        g0 += radial * x0 + B * (ln.x * xfm + fm.x * lnx + lm.x * xfn + fn.x * lmx);
-                        g1 += radial * x1 + B * (ln.y * xfm + fm.y * lnx + lm.y * xfn + fn.y * lmx);
-                        g2 += radial * x2 + B * (ln.z * xfm + fm.z * lnx + lm.z * xfn + fn.z * lmx);
-                        const T bl = B * lmx;
-                        v0 += A * lm.x + bl * x0;
-                        v1 += A * lm.y + bl * x1;
-                        v2 += A * lm.z + bl * x2;
-                    }
-                }
+        T v0 = 0, v1 = 0, v2 = 0;
+        if (sub == 0) {
+            v0 = c.self * ln.x;
+            v1 = c.self * ln.y;
+            v2 = c.self * ln.z;
+        }
+        for (int q = sub; q < 27; q += TPP) {
+            const int nz = imod(cz + q / 9 - 1, c.m2);
+            const int ny = imod(cy + (q / 3) % 3 - 1, c.m1);
+            const int nx = imod(cx + q % 3 - 1, c.m0);
+            const int cn = nx + (ny + nz * c.m1) * c.m0;
+            const int e = off[cn + 1];
+            for (int s2 = off[cn]; s2 < e; ++s2) {
+                if (s2 == s) continue;
+                const vec4<T> ym = Ys[s2];
+                const T x0 = min_image(sub_rn(yn.x, ym.x), c.L0);
+                const T x1 = min_image(sub_rn(yn.y, ym.y), c.L1);
+                const T x2 = min_image(sub_rn(yn.z, ym.z), c.L2);
+                const T rr = add_rn(add_rn(mul_rn(x0, x0), mul_rn(x1, x1)), mul_rn(x2, x2));
+                if (!(rr < c.Rc2)) continue;
+                const T r = sqrt_t(rr);
+                T A, B, dA, dB;
+                correction_scalars_d(r, c, cg, A, B, dA, dB);
+                const vec4<T> fm = Fs[s2], lm = Ls[s2];
+                const T lnx = ln.x * x0 + ln.y * x1 + ln.z * x2;
+                const T lmx = lm.x * x0 + lm.y * x1 + lm.z * x2;
+                const T xfm = x0 * fm.x + x1 * fm.y + x2 * fm.z;
+                const T xfn = x0 * fn.x + x1 * fn.y + x2 * fn.z;
+                const T P = ln.x * fm.x + ln.y * fm.y + ln.z * fm.z + lm.x * fn.x + lm.y * fn.y +
+                            lm.z * fn.z;
+                const T radial = (dA * P + dB * (lnx * xfm + lmx * xfn)) / r;
+                g0 += radial * x0 + B * (ln.x * xfm + fm.x * lnx + lm.x * xfn + fn.x * lmx);
+                g1 += radial * x1 + B * (ln.y * xfm + fm.y * lnx + lm.y * xfn + fn.y * lmx);
+                g2 += radial * x2 + B * (ln.z * xfm + fm.z * lnx + lm.z * xfn + fn.z * lmx);
+                const T bl = B * lmx;
+                v0 += A * lm.x + bl * x0;
+                v1 += A * lm.y + bl * x1;
+                v2 += A * lm.z + bl * x2;
             }
         }
-        const int64_t n = perm[s];
-        dY[3 * n] += g0;
-        dY[3 * n + 1] += g1;
-        dY[3 * n + 2] += g2;
-        dF[3 * n] += v0;
-        dF[3 * n + 1] += v1;
-        dF[3 * n + 2] += v2;
+#pragma unroll
+        for (int o = 1; o < TPP; o <<= 1) {
+            g0 += __shfl_xor_sync(group, g0, o);
+            g1 += __shfl_xor_sync(group, g1, o);
+            g2 += __shfl_xor_sync(group, g2, o);
+            v0 += __shfl_xor_sync(group, v0, o);
+            v1 += __shfl_xor_sync(group, v1, o);
+            v2 += __shfl_xor_sync(group, v2, o);
+        }
+        if (sub == 0) {
+            const int64_t n = perm[s];
+            dY[3 * n] += g0;
+            dY[3 * n + 1] += g1;
+            dY[3 * n + 2] += g2;
+            dF[3 * n] += v0;
+            dF[3 * n + 1] += v1;
+            dF[3 * n + 2] += v2;
+        }
     }
 }
 

@@ -7,9 +7,8 @@
 // hash order, 27 wrapped neighbour cells dz/dy/dx, s2 != s, r^2 < R_c^2,
 // V[:, original_index[s]] += v).
 //
-// One thread per sorted particle gathers over the 27 cells in the reference's
-// loop order, so the accumulation order per particle is the reference's; no
-// atomics. The separation, r^2 and the cutoff test use unfused IEEE
+// A few threads per sorted particle gather over the 27 cells (no atomics,
+// deterministic). The separation, r^2 and the cutoff test use unfused IEEE
 // operations, so the set of interacting pairs is exactly the reference's.
 #pragma once
 
@@ -54,15 +53,26 @@ __device__ __forceinline__ T min_image(T x, T L) {
     return sub_rn(x, mul_rn(L, rint_t(div_rn(x, L))));
 }
 
+// TPP threads per sorted particle share its 27 neighbour cells (cell q of the
+// reference's dz/dy/dx order goes to lane q mod TPP), so that small systems
+// still fill the GPU; the lanes' sums are combined by shuffles. Large systems
+// use one thread per particle (corr_tpp picks).
 // Vs == nullptr: V[:, perm[s]] += dv (the step API, reference semantics).
 // Vs != nullptr: V[:, perm[s]] = h3 * Vs[s] + dv (finishes the fused
 // interpolation, which left its sums in sorted order in Vs).
-template <typename T>
+inline int corr_tpp(int64_t n_part) { return n_part <= 200000 ? 4 : 1; }
+
+template <typename T, int TPP>
 __global__ void k_correct(int n_part, const vec4<T>* __restrict__ Ys,
                           const vec4<T>* __restrict__ Fs, const int32_t* __restrict__ off,
                           const int32_t* __restrict__ perm, T* __restrict__ V, CorrConsts<T> c,
                           const T* __restrict__ Vs, T h3) {
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n_part; s += gridDim.x * blockDim.x) {
+    const int sub = threadIdx.x % TPP;
+    const unsigned group = ((1u << TPP) - 1u) << (lane_id() & ~(TPP - 1));
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n_part * TPP;
+         t += nthreads) {
+        const int s = (int)(t / TPP);
         const vec4<T> yn = Ys[s];
         const vec4<T> fn = Fs[s];
         int cx = (int)floor_t(mul_rn(yn.x, c.ic0));
@@ -71,44 +81,61 @@ __global__ void k_correct(int n_part, const vec4<T>* __restrict__ Ys,
         cx = max(0, min(cx, c.m0 - 1));
         cy = max(0, min(cy, c.m1 - 1));
         cz = max(0, min(cz, c.m2 - 1));
-        T v0 = c.self * fn.x, v1 = c.self * fn.y, v2 = c.self * fn.z;
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int nz = imod(cz + dz, c.m2);
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int ny = imod(cy + dy, c.m1);
-                for (int dx = -1; dx <= 1; ++dx) {
-                    const int nx = imod(cx + dx, c.m0);
-                    const int cn = nx + (ny + nz * c.m1) * c.m0;
-                    const int e = off[cn + 1];
-                    for (int s2 = off[cn]; s2 < e; ++s2) {
-                        if (s2 == s) continue;
-                        const vec4<T> ym = Ys[s2];
-                        const T x0 = min_image(sub_rn(yn.x, ym.x), c.L0);
-                        const T x1 = min_image(sub_rn(yn.y, ym.y), c.L1);
-                        const T x2 = min_image(sub_rn(yn.z, ym.z), c.L2);
-                        const T rr = add_rn(add_rn(mul_rn(x0, x0), mul_rn(x1, x1)), mul_rn(x2, x2));
-                        if (!(rr < c.Rc2)) continue;
-                        T A, B;
-                        correction_scalars(sqrt_t(rr), c, A, B);
-                        const vec4<T> fm = Fs[s2];
-                        const T xF = x0 * fm.x + x1 * fm.y + x2 * fm.z;
-                        const T bx = B * xF;
-                        v0 += A * fm.x + bx * x0;
-                        v1 += A * fm.y + bx * x1;
-                        v2 += A * fm.z + bx * x2;
-                    }
-                }
-            }
+        T v0 = 0, v1 = 0, v2 = 0;
+        if (sub == 0) {
+            v0 = c.self * fn.x;
+            v1 = c.self * fn.y;
+            v2 = c.self * fn.z;
         }
-        const int64_t n = perm[s];
-        if (Vs) {
-            V[3 * n] = h3 * Vs[3 * (int64_t)s] + v0;
-            V[3 * n + 1] = h3 * Vs[3 * (int64_t)s + 1] + v1;
-            V[3 * n + 2] = h3 * Vs[3 * (int64_t)s + 2] + v2;
+        auto visit = [&](int nx, int ny, int nz) {
+            const int cn = nx + (ny + nz * c.m1) * c.m0;
+            const int e = off[cn + 1];
+            for (int s2 = off[cn]; s2 < e; ++s2) {
+                if (s2 == s) continue;
+                const vec4<T> ym = Ys[s2];
+                const T x0 = min_image(sub_rn(yn.x, ym.x), c.L0);
+                const T x1 = min_image(sub_rn(yn.y, ym.y), c.L1);
+                const T x2 = min_image(sub_rn(yn.z, ym.z), c.L2);
+                const T rr = add_rn(add_rn(mul_rn(x0, x0), mul_rn(x1, x1)), mul_rn(x2, x2));
+                if (!(rr < c.Rc2)) continue;
+                T A, B;
+                correction_scalars(sqrt_t(rr), c, A, B);
+                const vec4<T> fm = Fs[s2];
+                const T xF = x0 * fm.x + x1 * fm.y + x2 * fm.z;
+                const T bx = B * xF;
+                v0 += A * fm.x + bx * x0;
+                v1 += A * fm.y + bx * x1;
+                v2 += A * fm.z + bx * x2;
+            }
+        };
+        if constexpr (TPP == 1) {
+            // the reference's dz / dy / dx loop order
+            for (int dz = -1; dz <= 1; ++dz)
+                for (int dy = -1; dy <= 1; ++dy)
+                    for (int dx = -1; dx <= 1; ++dx)
+                        visit(imod(cx + dx, c.m0), imod(cy + dy, c.m1), imod(cz + dz, c.m2));
         } else {
-            V[3 * n] += v0;
-            V[3 * n + 1] += v1;
-            V[3 * n + 2] += v2;
+            // cell q of that order goes to lane q mod TPP
+            for (int q = sub; q < 27; q += TPP)
+                visit(imod(cx + q % 3 - 1, c.m0), imod(cy + (q / 3) % 3 - 1, c.m1), imod(cz + q / 9 - 1, c.m2));
+        }
+#pragma unroll
+        for (int o = 1; o < TPP; o <<= 1) {
+            v0 += __shfl_xor_sync(group, v0, o);
+            v1 += __shfl_xor_sync(group, v1, o);
+            v2 += __shfl_xor_sync(group, v2, o);
+        }
+        if (sub == 0) {
+            const int64_t n = perm[s];
+            if (Vs) {
+                V[3 * n] = h3 * Vs[3 * (int64_t)s] + v0;
+                V[3 * n + 1] = h3 * Vs[3 * (int64_t)s + 1] + v1;
+                V[3 * n + 2] = h3 * Vs[3 * (int64_t)s + 2] + v2;
+            } else {
+                V[3 * n] += v0;
+                V[3 * n + 1] += v1;
+                V[3 * n + 2] += v2;
+            }
         }
     }
 }

@@ -817,7 +817,7 @@ struct Engine final : EngineBase {
         }
         TRY(interp_from_spectrum(s));
         StageScope sc(h, FFCM_STAGE_CORRECT, s);
-        return launch(h, k_correct<T>, grid_for(N, 128), 128, 0, s, N, (const vec4<T>*)Ys,
+        return launch(h, corr_tpp(N) == 4 ? k_correct<T, 4> : k_correct<T, 1>, grid_for((int64_t)N * corr_tpp(N), 128), 128, 0, s, N, (const vec4<T>*)Ys,
                       (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
                       static_cast<T*>(V), cc, (const T*)partial, h3);
     }
@@ -890,7 +890,8 @@ struct Engine final : EngineBase {
                        (const T*)gu, (const T*)gpsi, static_cast<T*>(dY), static_cast<T*>(dF), sp, h3));
         }
         StageScope sc(h, FFCM_STAGE_CORRECT, s);
-        return launch(h, k_correct_adjoint<T>, grid_for(N, 128), 128, 0, s, N, (const vec4<T>*)Ys,
+        return launch(h, corr_tpp(N) == 4 ? k_correct_adjoint<T, 4> : k_correct_adjoint<T, 1>,
+                      grid_for((int64_t)N * corr_tpp(N), 128), 128, 0, s, N, (const vec4<T>*)Ys,
                       (const vec4<T>*)Fs, (const vec4<T>*)Ls, (const int32_t*)off, (const int32_t*)perm,
                       static_cast<T*>(dY), static_cast<T*>(dF), cc, cgc);
     }
@@ -992,7 +993,7 @@ struct Engine final : EngineBase {
 
     int correct(void* V, cudaStream_t s) override {
         StageScope sc(h, FFCM_STAGE_CORRECT, s);
-        return launch(h, k_correct<T>, grid_for(N, 128), 128, 0, s, N, (const vec4<T>*)Ys,
+        return launch(h, corr_tpp(N) == 4 ? k_correct<T, 4> : k_correct<T, 1>, grid_for((int64_t)N * corr_tpp(N), 128), 128, 0, s, N, (const vec4<T>*)Ys,
                       (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
                       static_cast<T*>(V), cc, (const T*)nullptr, T(0));
     }
