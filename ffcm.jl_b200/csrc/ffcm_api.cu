@@ -22,6 +22,7 @@
 #include "fft.cuh"
 #include "fft_dispatch.cuh"
 #include "fft_pipe.cuh"
+#include "fft_tma.cuh"
 #include "slab.cuh"
 #include "spread_interp.cuh"
 
@@ -68,6 +69,25 @@ int raise_smem_cap(const void* func, size_t bytes) {
     CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
     cur = bytes;
     return FFCM_OK;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library does not link the driver library itself).
+using TensorMapEncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                       const cuuint64_t*, const cuuint32_t*, const cuuint32_t*,
+                                       CUtensorMapInterleave, CUtensorMapSwizzle, CUtensorMapL2promotion,
+                                       CUtensorMapFloatOOBfill);
+
+TensorMapEncodeFn tensor_map_encoder() {
+    static TensorMapEncodeFn fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<TensorMapEncodeFn>(f);
+    }();
+    return fn;
 }
 
 std::string fmt(double v) {
@@ -319,6 +339,10 @@ struct Engine final : EngineBase {
     int ykind = 0, zkind = 0, ygrid = 0, zgrid = 0;
     // kx columns per chunk of the y/z/y passes (0: one pass over the spectrum)
     int kx_chunk = 0;
+    // tensor maps of the spectrum for the TMA z pass, one per bundle width B
+    // (index log2 B); valid[i] false where the map could not be made
+    CUtensorMap zmap[5];
+    bool zmap_ok[5] = {false, false, false, false, false};
     int num_sms = 148;
     size_t smem_fx = 0, smem_fy = 0, smem_fz = 0;
     // slab kernels: spread/interpolation fused with the x transforms
@@ -501,6 +525,8 @@ struct Engine final : EngineBase {
         for (int B : {2, 4, 8, 16}) {
             if (fast_y && ypipe_kernel<T>(My, B) && hxp % B == 0 && ypipe_smem<T>(My, B) <= budget)
                 TRY(raise_smem_cap((const void*)ypipe_kernel<T>(My, B), ypipe_smem<T>(My, B)));
+            if (fast_z && ztma_kernel<T>(Mz, B) && ztma_smem<T>(Mz, B) <= 226 * 1024)
+                TRY(raise_smem_cap((const void*)ztma_kernel<T>(Mz, B), ztma_smem<T>(Mz, B)));
             if (fast_z && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= budget)
                 TRY(raise_smem_cap((const void*)zlr_kernel<T>(Mz, B), FastFft<T>::zlr_smem(Mz, B)));
             if (fast_z && zpipe_kernel<T>(Mz, B) && hxp % B == 0 && zpipe_smem<T>(Mz, B) <= budget)
@@ -545,6 +571,7 @@ struct Engine final : EngineBase {
 
         // zero-initialised grids and cell list (src/config.jl:464-469)
         CUDA_TRY(cudaMemset(spec, 0, 3 * (size_t)hxp * My * Mz * sizeof(cplx<T>)));
+        if (fast_z) make_z_maps();
         CUDA_TRY(cudaMemset(off, 0, ((size_t)ncell + 1) * sizeof(int32_t)));
         CUDA_TRY(cudaMemset(perm, 0, (size_t)N * sizeof(int32_t)));
         CUDA_TRY(cudaMemset(key, 0, (size_t)N * sizeof(int32_t)));
@@ -615,6 +642,27 @@ struct Engine final : EngineBase {
         return FFCM_OK;
     }
 
+    // Spectrum as a 3-D tensor (kx, y, c * Mz + z) of 8-byte words, boxes of
+    // B kx columns x 1 y x min(256, Mz) rows.
+    void make_z_maps() {
+        TensorMapEncodeFn enc = tensor_map_encoder();
+        if (!enc) return;
+        constexpr int EPC = TmaElem<T>::PER_CPLX;
+        const cuuint64_t dims[3] = {(cuuint64_t)hxp * EPC, (cuuint64_t)My, (cuuint64_t)3 * Mz};
+        const cuuint64_t strides[2] = {(cuuint64_t)hxp * sizeof(cplx<T>), (cuuint64_t)My * hxp * sizeof(cplx<T>)};
+        const cuuint32_t estr[3] = {1, 1, 1};
+        for (int i = 1, B = 2; B <= 16; ++i, B *= 2) {
+            if (!ztma_kernel<T>(Mz, B) || hxp % B != 0) continue;
+            const cuuint32_t box[3] = {(cuuint32_t)(B * EPC), 1, (cuuint32_t)tma_zbox(Mz)};
+            zmap_ok[i] = enc(&zmap[i], sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                             3, spec, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        }
+    }
+
+    static int log2i(int B) { return B == 2 ? 1 : B == 4 ? 2 : B == 8 ? 3 : B == 16 ? 4 : 0; }
+
     int autotune() {
         const bool verbose = std::getenv("FFCM_VERBOSE") != nullptr;
         if (fast_y) {
@@ -649,12 +697,14 @@ struct Engine final : EngineBase {
         if (fast_z) {
             float best = 1e30f;
             int bk = 0, bB = Bz, bg = 0;
-            for (int kind = 0; kind < 3; ++kind)
+            for (int kind = 0; kind < 4; ++kind)
                 for (int B : {2, 4, 8, 16}) {
                     if (kind == 0 && !z_kernel<T>(Mz, B)) continue;
                     if (kind == 1 && !(zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
                                        zpipe_smem<T>(Mz, B) <= 200 * 1024)) continue;
                     if (kind == 2 && !(zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= 200 * 1024)) continue;
+                    if (kind == 3 && !(ztma_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
+                                       ztma_smem<T>(Mz, B) <= 226 * 1024)) continue;
                     if (kind == 0) {
                         int cand[4];
                         const int nc = z_bundles(Mz, cand);
@@ -668,6 +718,11 @@ struct Engine final : EngineBase {
                         const int ntiles = ((nkx + B - 1) / B) * My;
                         TRY(persistent_grid((const void*)zpipe_kernel<T>(Mz, B), B * (Mz / 8),
                                             zpipe_smem<T>(Mz, B), ntiles, zgrid));
+                    }
+                    if (kind == 3) {
+                        const int ntiles = ((nkx + B - 1) / B) * My;
+                        TRY(persistent_grid((const void*)ztma_kernel<T>(Mz, B), B * (Mz / 8),
+                                            ztma_smem<T>(Mz, B), ntiles, zgrid));
                     }
                     float ms = 0;
                     TRY(time_launches([&] { return launch_z(h->stream); }, ms));
@@ -922,6 +977,12 @@ struct Engine final : EngineBase {
 
     int launch_z(cudaStream_t s, int k0 = 0, int k1 = 0) {
         if (k1 <= 0) k1 = nkx;
+        if (fast_z && zkind == 3) {
+            const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
+            return launch(h, ztma_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), ztma_smem<T>(Mz, Bz), s,
+                          zmap[log2i(Bz)], spec, k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv,
+                          (const T*)kyv, (const T*)kzv, inv_mu_M, h->d_err);
+        }
         if (fast_z && zkind == 2) {
             dim3 g((k1 - k0 + Bz - 1) / Bz, My, 1);
             return launch(h, zlr_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::zlr_smem(Mz, Bz), s, spec,

@@ -1,0 +1,147 @@
+// z pass + projector with tiles brought in by the tensor memory accelerator.
+//
+// Same computation as k_fftq_z_stokes (z forward of the three components in
+// lockstep, projector (I - k k^T/k^2)/(mu k^2 M), z inverse). A persistent
+// block loops over tiles of B kx columns x one y x all (c, z) rows. One thread
+// loads a tile with a few tiled bulk copies (cp.async.bulk.tensor) described
+// by a tensor map over the spectrum, dims (kx, y, 3 Mz) -- the component and
+// z axes merge because a component's stride is Mz times the z stride -- into
+// a staging buffer, completing on an mbarrier; as soon as the block has moved
+// the tile into registers, the next tile's copy is issued, so it lands while
+// the block transforms. Each block fills only its own shared memory, from this
+// GPU's memory. The x coordinate of every copy is a multiple of B complex
+// values (B even), so it starts on a 16-byte boundary.
+#pragma once
+
+#include <cuda.h>
+
+#include "bulk_copy.cuh"
+#include "common.cuh"
+#include "fft_pipe.cuh"
+
+namespace ffcm {
+
+// Tensor-map element: 8-byte words; a complex value is 1 (float) or 2 (double).
+template <typename T>
+struct TmaElem {
+    static constexpr int PER_CPLX = (int)(sizeof(cplx<T>) / 8);
+};
+
+// Rows of (c, z) per tiled copy (box dimensions are at most 256).
+__host__ __device__ constexpr int tma_zbox(int n) { return n < 256 ? n : 256; }
+
+__device__ __forceinline__ void tma_load_3d(void* dst_smem, const CUtensorMap* map, int x, int y, int z,
+                                            uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst_smem)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// block = B * n/8 threads; smem: up to 128 bytes of alignment slack | staging
+// (3 n B, 128-byte aligned) | table (n) | exchange (3 B padded_len(n)).
+template <typename T, int n, int B>
+__global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
+    const __grid_constant__ CUtensorMap tmap, cplx<T>* __restrict__ spec, int kx0, int kx1, int My, int hxp,
+    const cplx<T>* __restrict__ twz, const T* __restrict__ kxv, const T* __restrict__ kyv,
+    const T* __restrict__ kzv, T inv_mu_M, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    constexpr int Q = n / 8, PL = padded_len(n), ZB = tma_zbox(n), NCOPY = 3 * n / ZB;
+    constexpr unsigned TILE_BYTES = (unsigned)(3 * n * B * sizeof(cplx<T>));
+    // staging starts on a 128-byte boundary (the size includes 128 bytes of slack)
+    cplx<T>* stage = reinterpret_cast<cplx<T>*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    cplx<T>* tw = stage + 3 * n * B;
+    cplx<T>* ex_sm = tw + n;
+    load_table(tw, twz, n);
+    const int b = threadIdx.x % B, j = threadIdx.x / B;
+    const int tiles_x = (kx1 - kx0 + B - 1) / B;
+    const int ntiles = tiles_x * My;
+    const int64_t zs = (int64_t)My * hxp;
+    const int64_t cs = (int64_t)n * zs;
+    auto issue = [&](int t) {   // one thread
+        const int tx = t % tiles_x, y = t / tiles_x;
+        mbar_arrive_expect(&bar, TILE_BYTES);
+#pragma unroll
+        for (int k = 0; k < NCOPY; ++k)
+            tma_load_3d(stage + k * ZB * B, &tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, y, k * ZB, &bar);
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        if ((int)blockIdx.x < ntiles) issue(blockIdx.x);
+    }
+    __syncthreads();
+    const Exchange<T> ex[3] = {Exchange<T>{ex_sm, b, B}, Exchange<T>{ex_sm + B * PL, b, B},
+                               Exchange<T>{ex_sm + 2 * B * PL, b, B}};
+    unsigned phase = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
+        const bool landed = mbar_wait_bounded(&bar, phase, 1 << 22);
+        if (__syncthreads_or(!landed)) {
+            // the tile did not arrive: report, give the copies one more
+            // bounded chance to finish, and leave
+            if (threadIdx.x == 0) atomicOr(err, DEVERR_COPY_TIMEOUT);
+            mbar_wait_bounded(&bar, phase, 1 << 22);
+            return;
+        }
+        cplx<T> v[3][8];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[c][q] = stage[(c * n + j + q * Q) * B + b];
+        __syncthreads();   // the staging buffer is free for the next tile
+        if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
+        const int tx = t % tiles_x, y = t / tiles_x;
+        const int kx = kx0 + tx * B + b;
+        fft_lines_lockstep<T, n, 3>(v, j, ex, tw, false);
+        const T k1 = kx < kx1 ? kxv[kx] : T(0);
+        const T k2 = kyv[y];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const T k3 = kzv[j + q * Q];
+            const T ksq = k1 * k1 + k2 * k2 + k3 * k3;
+            if (ksq == T(0)) {
+                v[0][q] = v[1][q] = v[2][q] = cplx<T>{T(0), T(0)};
+            } else {
+                const T inv_k2 = T(1) / ksq;
+                const T sc = inv_mu_M * inv_k2;
+                const T dre = (k1 * v[0][q].x + k2 * v[1][q].x + k3 * v[2][q].x) * inv_k2;
+                const T dim = (k1 * v[0][q].y + k2 * v[1][q].y + k3 * v[2][q].y) * inv_k2;
+                v[0][q] = cplx<T>{sc * (v[0][q].x - k1 * dre), sc * (v[0][q].y - k1 * dim)};
+                v[1][q] = cplx<T>{sc * (v[1][q].x - k2 * dre), sc * (v[1][q].y - k2 * dim)};
+                v[2][q] = cplx<T>{sc * (v[2][q].x - k3 * dre), sc * (v[2][q].y - k3 * dim)};
+            }
+        }
+        fft_lines_lockstep<T, n, 3>(v, j, ex, tw, true);
+        if (kx < kx1) {
+            cplx<T>* col = spec + (int64_t)y * hxp + kx;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int64_t o = (int64_t)(j + q * Q) * zs;
+                col[o] = v[0][q];
+                col[cs + o] = v[1][q];
+                col[2 * cs + o] = v[2][q];
+            }
+        }
+    }
+}
+
+template <typename T>
+using ZTmaKernel = void (*)(const CUtensorMap, cplx<T>*, int, int, int, int, const cplx<T>*, const T*,
+                            const T*, const T*, T, int*);
+
+template <typename T>
+size_t ztma_smem(int n, int B) {
+    return 128 + (size_t)(3 * n * B + n + 3 * B * padded_len(n)) * sizeof(cplx<T>);
+}
+
+template <typename T>
+ZTmaKernel<T> ztma_kernel(int n, int B) {
+#define FFCM_ZT(NN, BB) if (n == NN && B == BB) return k_fftt_z_stokes<T, NN, BB>;
+    FFCM_ZT(64, 8) FFCM_ZT(64, 16) FFCM_ZT(128, 4) FFCM_ZT(128, 8) FFCM_ZT(256, 2) FFCM_ZT(256, 4)
+    FFCM_ZT(512, 2) FFCM_ZT(512, 4) FFCM_ZT(512, 8) FFCM_ZT(1024, 2)
+#undef FFCM_ZT
+    return nullptr;
+}
+
+}  // namespace ffcm
