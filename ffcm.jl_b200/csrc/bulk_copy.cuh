@@ -43,6 +43,14 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
     return false;
 }
 
+// Orders this thread's earlier shared-memory accesses, and those of other
+// threads made visible to it by a barrier, before later bulk copies (the copy
+// engine is another proxy): needed before a copy overwrites shared memory that
+// threads have just read.
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // global -> shared, completing `bytes` of transactions on `bar`.
 __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_global, unsigned bytes, uint64_t* bar) {
     asm volatile(

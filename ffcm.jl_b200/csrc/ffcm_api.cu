@@ -343,6 +343,8 @@ struct Engine final : EngineBase {
     // (index log2 B); valid[i] false where the map could not be made
     CUtensorMap zmap[5];
     bool zmap_ok[5] = {false, false, false, false, false};
+    CUtensorMap ymap[5];   // same, boxes for the TMA y pass
+    bool ymap_ok[5] = {false, false, false, false, false};
     int num_sms = 148;
     size_t smem_fx = 0, smem_fy = 0, smem_fz = 0;
     // slab kernels: spread/interpolation fused with the x transforms
@@ -525,6 +527,8 @@ struct Engine final : EngineBase {
         for (int B : {2, 4, 8, 16}) {
             if (fast_y && ypipe_kernel<T>(My, B) && hxp % B == 0 && ypipe_smem<T>(My, B) <= budget)
                 TRY(raise_smem_cap((const void*)ypipe_kernel<T>(My, B), ypipe_smem<T>(My, B)));
+            if (fast_y && ytma_kernel<T>(My, B) && ytma_smem<T>(My, B) <= 226 * 1024)
+                TRY(raise_smem_cap((const void*)ytma_kernel<T>(My, B), ytma_smem<T>(My, B)));
             if (fast_z && ztma_kernel<T>(Mz, B) && ztma_smem<T>(Mz, B) <= 226 * 1024)
                 TRY(raise_smem_cap((const void*)ztma_kernel<T>(Mz, B), ztma_smem<T>(Mz, B)));
             if (fast_z && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= budget)
@@ -571,7 +575,7 @@ struct Engine final : EngineBase {
 
         // zero-initialised grids and cell list (src/config.jl:464-469)
         CUDA_TRY(cudaMemset(spec, 0, 3 * (size_t)hxp * My * Mz * sizeof(cplx<T>)));
-        if (fast_z) make_z_maps();
+        if (fast_z || fast_y) make_tma_maps();
         CUDA_TRY(cudaMemset(off, 0, ((size_t)ncell + 1) * sizeof(int32_t)));
         CUDA_TRY(cudaMemset(perm, 0, (size_t)N * sizeof(int32_t)));
         CUDA_TRY(cudaMemset(key, 0, (size_t)N * sizeof(int32_t)));
@@ -644,35 +648,58 @@ struct Engine final : EngineBase {
 
     // Spectrum as a 3-D tensor (kx, y, c * Mz + z) of 8-byte words, boxes of
     // B kx columns x 1 y x min(256, Mz) rows.
-    void make_z_maps() {
+    // Spectrum as a 3-D tensor (kx, y, c * Mz + z) of 8-byte words. z pass:
+    // boxes of B kx columns x 1 y x min(256, Mz) rows; y pass: B kx columns x
+    // min(256, My) rows x 1 plane.
+    void make_tma_maps() {
         TensorMapEncodeFn enc = tensor_map_encoder();
         if (!enc) return;
         constexpr int EPC = TmaElem<T>::PER_CPLX;
         const cuuint64_t dims[3] = {(cuuint64_t)hxp * EPC, (cuuint64_t)My, (cuuint64_t)3 * Mz};
         const cuuint64_t strides[2] = {(cuuint64_t)hxp * sizeof(cplx<T>), (cuuint64_t)My * hxp * sizeof(cplx<T>)};
         const cuuint32_t estr[3] = {1, 1, 1};
+        const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+        auto make = [&](CUtensorMap* m, cuuint32_t bx, cuuint32_t by, cuuint32_t bz) {
+            const cuuint32_t box[3] = {bx, by, bz};
+            return enc(m, dt, 3, spec, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                       CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+        };
         for (int i = 1, B = 2; B <= 16; ++i, B *= 2) {
-            if (!ztma_kernel<T>(Mz, B) || hxp % B != 0) continue;
-            const cuuint32_t box[3] = {(cuuint32_t)(B * EPC), 1, (cuuint32_t)tma_zbox(Mz)};
-            zmap_ok[i] = enc(&zmap[i], sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                             3, spec, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+            if (hxp % B != 0) continue;
+            if (fast_z && ztma_kernel<T>(Mz, B))
+                zmap_ok[i] = make(&zmap[i], (cuuint32_t)(B * EPC), 1, (cuuint32_t)tma_zbox(Mz));
+            if (fast_y && ytma_kernel<T>(My, B))
+                ymap_ok[i] = make(&ymap[i], (cuuint32_t)(B * EPC), (cuuint32_t)tma_zbox(My), 1);
         }
     }
 
     static int log2i(int B) { return B == 2 ? 1 : B == 4 ? 2 : B == 8 ? 3 : B == 16 ? 4 : 0; }
 
+    // "kind,B" from an environment variable: pins the autotuner to one
+    // variant (tests use it to run every variant); -1 when unset.
+    static void forced_variant(const char* name, int& kind, int& B) {
+        kind = B = -1;
+        const char* v = std::getenv(name);
+        if (v && std::sscanf(v, "%d,%d", &kind, &B) != 2) kind = B = -1;
+    }
+
     int autotune() {
         const bool verbose = std::getenv("FFCM_VERBOSE") != nullptr;
+        int fyk, fyB, fzk, fzB;
+        forced_variant("FFCM_FORCE_Y", fyk, fyB);
+        forced_variant("FFCM_FORCE_Z", fzk, fzB);
         if (fast_y) {
             float best = 1e30f;
             int bk = 0, bB = By, bg = 0;
-            for (int kind = 0; kind < 2; ++kind)
+            for (int kind = 0; kind < 3; ++kind)
                 for (int B : {2, 4, 8, 16}) {
+                    if (fyk >= 0 && (kind != fyk || B != fyB)) continue;
                     if (kind == 0 && !y_kernel<T>(My, B)) continue;
                     if (kind == 1 && !(ypipe_kernel<T>(My, B) && hxp % B == 0 &&
                                        ypipe_smem<T>(My, B) <= 200 * 1024)) continue;
+                    if (kind == 2 && !(ytma_kernel<T>(My, B) && ymap_ok[log2i(B)] &&
+                                       ytma_smem<T>(My, B) <= 226 * 1024)) continue;
                     if (kind == 0) {
                         int cand[4];
                         const int nc = y_bundles(My, cand);
@@ -687,11 +714,17 @@ struct Engine final : EngineBase {
                         TRY(persistent_grid((const void*)ypipe_kernel<T>(My, B), B * (My / 8),
                                             ypipe_smem<T>(My, B), ntiles, ygrid));
                     }
+                    if (kind == 2) {
+                        const int ntiles = ((nkx + B - 1) / B) * Mz * 3;
+                        TRY(persistent_grid((const void*)ytma_kernel<T>(My, B), B * (My / 8),
+                                            ytma_smem<T>(My, B), ntiles, ygrid));
+                    }
                     float ms = 0;
                     TRY(time_launches([&] { return launch_y(h->stream, 0); }, ms));
                     if (verbose) fprintf(stderr, "ffcm autotune: y n=%d kind=%d B=%d %.4f ms\n", My, kind, B, ms / 3);
                     if (ms < best) { best = ms; bk = kind; bB = B; bg = ygrid; }
                 }
+            if (fyk >= 0 && best == 1e30f) return fail(FFCM_ERR_ARGUMENT, "FFCM_FORCE_Y names no available y variant");
             ykind = bk; By = bB; ygrid = bg;
         }
         if (fast_z) {
@@ -699,6 +732,7 @@ struct Engine final : EngineBase {
             int bk = 0, bB = Bz, bg = 0;
             for (int kind = 0; kind < 4; ++kind)
                 for (int B : {2, 4, 8, 16}) {
+                    if (fzk >= 0 && (kind != fzk || B != fzB)) continue;
                     if (kind == 0 && !z_kernel<T>(Mz, B)) continue;
                     if (kind == 1 && !(zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
                                        zpipe_smem<T>(Mz, B) <= 200 * 1024)) continue;
@@ -729,6 +763,7 @@ struct Engine final : EngineBase {
                     if (verbose) fprintf(stderr, "ffcm autotune: z n=%d kind=%d B=%d %.4f ms\n", Mz, kind, B, ms / 3);
                     if (ms < best) { best = ms; bk = kind; bB = B; bg = zgrid; }
                 }
+            if (fzk >= 0 && best == 1e30f) return fail(FFCM_ERR_ARGUMENT, "FFCM_FORCE_Z names no available z variant");
             zkind = bk; Bz = bB; zgrid = bg;
         }
         if (fast_y && fast_z) {
@@ -736,7 +771,10 @@ struct Engine final : EngineBase {
             const double col_bytes = 3.0 * My * Mz * sizeof(cplx<T>);
             float best = 1e30f;
             int bc = 0;
+            const char* fc = std::getenv("FFCM_FORCE_CHUNK");
+            const int force_c = fc ? std::atoi(fc) : -1;
             for (int c : {0, 64, 32, 16, 8, 4}) {
+                if (force_c >= 0 && c != force_c) continue;
                 if (c > 0 && (c % By != 0 || c % Bz != 0 || c >= nkx || c * col_bytes > 96e6)) continue;
                 kx_chunk = c;
                 float ms = 0;
@@ -744,6 +782,8 @@ struct Engine final : EngineBase {
                 if (verbose) fprintf(stderr, "ffcm autotune: yz chunk=%d %.4f ms\n", c, ms / 3);
                 if (ms < best) { best = ms; bc = c; }
             }
+            if (force_c > 0 && best == 1e30f)
+                return fail(FFCM_ERR_ARGUMENT, "FFCM_FORCE_CHUNK names no available chunk width");
             kx_chunk = bc;
         }
         CUDA_TRY(cudaStreamSynchronize(h->stream));
@@ -960,6 +1000,11 @@ struct Engine final : EngineBase {
     // y pass over the kx columns [k0, k1) (the whole spectrum when k1 <= 0).
     int launch_y(cudaStream_t s, int inverse, int k0 = 0, int k1 = 0) {
         if (k1 <= 0) k1 = nkx;
+        if (fast_y && ykind == 2) {
+            const int ntiles = ((k1 - k0 + By - 1) / By) * Mz * 3;
+            return launch(h, ytma_kernel<T>(My, By), std::min(ygrid, ntiles), By * (My / 8), ytma_smem<T>(My, By),
+                          s, ymap[log2i(By)], spec, k0, k1, Mz, hxp, (const cplx<T>*)twy, inverse, h->d_err);
+        }
         if (fast_y && ykind == 1) {
             const int ntiles = ((k1 - k0 + By - 1) / By) * Mz * 3;
             return launch(h, ypipe_kernel<T>(My, By), std::min(ygrid, ntiles), By * (My / 8), ypipe_smem<T>(My, By),

@@ -1,4 +1,5 @@
-// z pass + projector with tiles brought in by the tensor memory accelerator.
+// y pass and z pass + projector with tiles brought in by the tensor memory
+// accelerator.
 //
 // Same computation as k_fftq_z_stokes (z forward of the three components in
 // lockstep, projector (I - k k^T/k^2)/(mu k^2 M), z inverse). A persistent
@@ -60,8 +61,9 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
     const int ntiles = tiles_x * My;
     const int64_t zs = (int64_t)My * hxp;
     const int64_t cs = (int64_t)n * zs;
-    auto issue = [&](int t) {   // one thread
+    auto issue = [&](int t) {   // one thread, after a barrier
         const int tx = t % tiles_x, y = t / tiles_x;
+        fence_proxy_async_smem();   // the block's reads of the staging buffer come first
         mbar_arrive_expect(&bar, TILE_BYTES);
 #pragma unroll
         for (int k = 0; k < NCOPY; ++k)
@@ -124,6 +126,83 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
             }
         }
     }
+}
+
+// y pass, same scheme: a tile is B kx columns x all n rows y of one (c, z)
+// plane (tensor coordinate z = c * Mz + z), loaded with n / min(256, n) tiled
+// copies into staging laid out [y][B].
+// block = B * n/8 threads; smem: slack | staging (n B) | table (n) | exchange (B padded_len(n)).
+template <typename T, int n, int B>
+__global__ void __launch_bounds__(B * (n / 8)) k_fftt_y(const __grid_constant__ CUtensorMap tmap,
+                                                        cplx<T>* __restrict__ spec, int kx0, int kx1, int Mz,
+                                                        int hxp, const cplx<T>* __restrict__ twy, int inverse,
+                                                        int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    constexpr int Q = n / 8, YB = tma_zbox(n), NCOPY = n / YB;
+    constexpr unsigned TILE_BYTES = (unsigned)(n * B * sizeof(cplx<T>));
+    cplx<T>* stage = reinterpret_cast<cplx<T>*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    cplx<T>* tw = stage + n * B;
+    cplx<T>* ex_sm = tw + n;
+    load_table(tw, twy, n);
+    const int b = threadIdx.x % B, j = threadIdx.x / B;
+    const int tiles_x = (kx1 - kx0 + B - 1) / B;
+    const int ntiles = tiles_x * Mz * 3;
+    const int64_t plane_elems = (int64_t)n * hxp;
+    auto issue = [&](int t) {   // one thread, after a barrier
+        const int tx = t % tiles_x, pz = t / tiles_x;
+        fence_proxy_async_smem();   // the block's reads of the staging buffer come first
+        mbar_arrive_expect(&bar, TILE_BYTES);
+#pragma unroll
+        for (int k = 0; k < NCOPY; ++k)
+            tma_load_3d(stage + k * YB * B, &tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, k * YB, pz, &bar);
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        if ((int)blockIdx.x < ntiles) issue(blockIdx.x);
+    }
+    __syncthreads();
+    const Exchange<T> ex[1] = {Exchange<T>{ex_sm, b, B}};
+    unsigned phase = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
+        const bool landed = mbar_wait_bounded(&bar, phase, 1 << 22);
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0) atomicOr(err, DEVERR_COPY_TIMEOUT);
+            mbar_wait_bounded(&bar, phase, 1 << 22);
+            return;
+        }
+        cplx<T> v[1][8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[0][q] = stage[(j + q * Q) * B + b];
+        __syncthreads();   // the staging buffer is free for the next tile
+        if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
+        fft_lines_lockstep<T, n, 1>(v, j, ex, tw, inverse != 0);
+        const int tx = t % tiles_x, pz = t / tiles_x;
+        const int kx = kx0 + tx * B + b;
+        if (kx < kx1) {
+            cplx<T>* dst = spec + (int64_t)pz * plane_elems + kx;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) dst[(int64_t)(j + q * Q) * hxp] = v[0][q];
+        }
+    }
+}
+
+template <typename T>
+using YTmaKernel = void (*)(const CUtensorMap, cplx<T>*, int, int, int, int, const cplx<T>*, int, int*);
+
+template <typename T>
+size_t ytma_smem(int n, int B) {
+    return 128 + (size_t)(n * B + n + B * padded_len(n)) * sizeof(cplx<T>);
+}
+
+template <typename T>
+YTmaKernel<T> ytma_kernel(int n, int B) {
+#define FFCM_YT(NN, BB) if (n == NN && B == BB) return k_fftt_y<T, NN, BB>;
+    FFCM_YT(32, 8) FFCM_YT(32, 16) FFCM_YT(64, 8) FFCM_YT(64, 16) FFCM_YT(128, 8) FFCM_YT(128, 16)
+    FFCM_YT(256, 4) FFCM_YT(256, 8) FFCM_YT(256, 16) FFCM_YT(512, 4) FFCM_YT(512, 8) FFCM_YT(512, 16)
+    FFCM_YT(1024, 4) FFCM_YT(1024, 8)
+#undef FFCM_YT
+    return nullptr;
 }
 
 template <typename T>

@@ -1,0 +1,78 @@
+"""Every launch variant the autotuner can choose computes the same solve.
+
+The autotuner keeps whichever y-pass, z-pass and kx-chunk variant is fastest
+on the machine at hand, so a parity test only ever sees the winner. Here
+each variant is pinned in turn (FFCM_FORCE_Y / FFCM_FORCE_Z = "kind,B",
+FFCM_FORCE_CHUNK = columns) and the solve compared with the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+import ffcm_oracle as O
+from fixtures import nonoverlapping_uniform
+from gpu_helpers import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+CASES = {"64^3": dict(L=(40.0,) * 3, N=2000, M=(64, 64, 64)),
+         "128^3": dict(L=(60.0,) * 3, N=5000, M=(128, 128, 128)),
+         "64x32x32": dict(L=(32.0, 16.0, 16.0), N=300, M=(64, 32, 32))}
+Y_VARIANTS = [(k, B) for k in (0, 1, 2) for B in (2, 4, 8, 16)]
+Z_VARIANTS = [(k, B) for k in (0, 1, 2, 3) for B in (2, 4, 8, 16)]
+
+
+def _solve(ffcm, T, case, env):
+    c = CASES[case]
+    kw = dict(L=c["L"], R_c=3.0 if case != "64x32x32" else 2.0, N=c["N"], kernel_widths_ratio=2.0,
+              viscosity=1.0, num_grid_points=c["M"], M_G=8)
+    old = {k: os.environ.get(k) for k in env}
+    os.environ.update(env)
+    try:
+        cfg = ffcm.FFCMConfig(T, **kw)
+    finally:
+        for k, v in old.items():
+            if v is None:
+                os.environ.pop(k, None)
+            else:
+                os.environ[k] = v
+    rng = np.random.default_rng(c["N"])
+    Y = nonoverlapping_uniform(c["N"], c["L"], 3).astype(T)
+    F = rng.standard_normal((c["N"], 3)).astype(T)
+    V = np.empty_like(Y)
+    ffcm.mobility(V, cfg, Y, F)
+    ora = O.OracleConfig(T, **kw)
+    return rel_l2(V, O.apply(ora, Y, F))
+
+
+def _check(ffcm, T, case, env):
+    try:
+        err = _solve(ffcm, T, case, env)
+    except ffcm.ArgumentError:
+        pytest.skip("variant not available for this configuration")
+    assert err < (1e-5 if T == np.float32 else 1e-10), (env, err)
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("kind,B", Y_VARIANTS)
+def test_y_variant(ffcm, T, case, kind, B):
+    _check(ffcm, T, case, {"FFCM_FORCE_Y": f"{kind},{B}", "FFCM_FORCE_CHUNK": "0"})
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+@pytest.mark.parametrize("case", list(CASES))
+@pytest.mark.parametrize("kind,B", Z_VARIANTS)
+def test_z_variant(ffcm, T, case, kind, B):
+    _check(ffcm, T, case, {"FFCM_FORCE_Z": f"{kind},{B}", "FFCM_FORCE_CHUNK": "0"})
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+@pytest.mark.parametrize("case", ["64^3", "128^3"])
+@pytest.mark.parametrize("chunk", [8, 16, 32])
+@pytest.mark.parametrize("pin", ["fastest", "tma"])
+def test_chunked_yz(ffcm, T, case, chunk, pin):
+    env = {"FFCM_FORCE_CHUNK": str(chunk)}
+    if pin == "tma":
+        env.update({"FFCM_FORCE_Y": "2,8", "FFCM_FORCE_Z": "3,8"})
+    _check(ffcm, T, case, env)
