@@ -373,6 +373,11 @@ class FFCMMobility:
     computes ``alpha*M*f + beta*v`` (beta = 0 overwrites v, ignoring NaN
     contents), ``M @ F`` maps a 3xN force array to a fresh velocity array.
     Symmetric positive-definite by construction.
+
+    The positions are fixed once: their cell list is built at construction
+    (``ffcm_set_positions``) and every application only re-gathers the forces
+    (``ffcm_mobility_apply``). If another solve ran on ``config`` in between,
+    the positions are fixed again before the application.
     """
 
     def __init__(self, config: FFCMConfig, Y):
@@ -387,6 +392,20 @@ class FFCMMobility:
         self.Y = np.ascontiguousarray(Y, config.T).copy()
         self.F_scratch = np.empty((config.N, 3), config.T)
         self.V_scratch = np.empty((config.N, 3), config.T)
+        self._set_positions()
+
+    def _set_positions(self):
+        _raise(L_.load().ffcm_set_positions(self.config.handle, self.Y.ctypes.data, L_.HOST, None))
+
+    def _apply(self, V, F):
+        """V = M F for (N, 3) host arrays of the config's type."""
+        lib = L_.load()
+        code = lib.ffcm_mobility_apply(self.config.handle, V.ctypes.data, F.ctypes.data, L_.HOST, None)
+        if code == L_.ERR_STATE:     # the config solved something else since
+            self._set_positions()
+            code = lib.ffcm_mobility_apply(self.config.handle, V.ctypes.data, F.ctypes.data, L_.HOST, None)
+        _raise(code)
+        return V
 
     @property
     def shape(self):
@@ -406,7 +425,7 @@ class FFCMMobility:
     def mul(self, v, f, alpha=None, beta=None):
         T = self.config.T
         self.F_scratch[...] = np.asarray(f, T).reshape(self.config.N, 3)
-        mobility(self.V_scratch, self.config, self.Y, self.F_scratch)
+        self._apply(self.V_scratch, self.F_scratch)
         out = self.V_scratch.reshape(-1)
         if alpha is None and beta is None:
             v[...] = out
@@ -420,8 +439,11 @@ class FFCMMobility:
         return v
 
     def __matmul__(self, F):
+        F = np.asarray(F)
+        if len(F.shape) != 2 or _julia_size(F) != (3, self.config.N):
+            raise DimensionMismatch(f"F must be 3xN for the config's N = {self.config.N}")
         V = np.empty((self.config.N, 3), self.config.T)
-        return mobility(V, self.config, self.Y, F)
+        return self._apply(V, np.ascontiguousarray(F, self.config.T))
 
     __mul__ = __matmul__
 

@@ -83,6 +83,8 @@ SIGNATURES = {
     "ffcm_adjoint": (_c.c_int, [_vp, _vp, _vp, _vp, _i32, _vp]),
     "ffcm_objective_gradient": (_c.c_int, [_vp, _dp, _vp, _vp, _vp, _vp, _vp, _vp, _i32, _vp]),
     "ffcm_sort_cells_noalloc": (_c.c_int, [_vp, _i64, _i32, _vp, _vp, _vp, _vp]),
+    "ffcm_set_positions": (_c.c_int, [_vp, _vp, _i32, _vp]),
+    "ffcm_mobility_apply": (_c.c_int, [_vp, _vp, _vp, _i32, _vp]),
 }
 
 _lib = None

@@ -2,6 +2,7 @@
 // the assembled operator, buffer access and measurement. See
 // include/ffcm_b200.h for the contract of every entry point.
 #include <algorithm>
+#include <array>
 #include <limits>
 #include <cmath>
 #include <cstdio>
@@ -233,6 +234,11 @@ struct EngineBase {
     // a further right-hand side on the positions of the last solve (the
     // cell list and the slab particle lists are reused)
     virtual int mobility_rest_same_positions(void* V, cudaStream_t s) = 0;
+    // fixed-position operator: the forces are re-gathered into the cached
+    // cell order and solved (the first solve after a new cell list also
+    // builds the slab lists)
+    virtual int apply_fixed(void* V, const void* F, cudaStream_t s) = 0;
+    bool lists_built = false;
     virtual int gather_forces(const void* F, cudaStream_t s) = 0;
     virtual int forward_checkpoint(void* V, cudaStream_t s) = 0;
     virtual int adjoint(const void* lam, void* dY, void* dF, cudaStream_t s) = 0;
@@ -264,6 +270,9 @@ struct ffcm_handle {
     // true while the state of the last ffcm_mobility_checkpoint (cell list,
     // sorted Y/F, velocity grid) is intact for ffcm_adjoint
     bool ckpt = false;
+    // true while the cell list of the last ffcm_set_positions is intact for
+    // ffcm_mobility_apply
+    bool positions = false;
     // profiling
     bool profiling = false;
     std::vector<cudaEvent_t> events;
@@ -684,11 +693,45 @@ struct Engine final : EngineBase {
         if (v && std::sscanf(v, "%d,%d", &kind, &B) != 2) kind = B = -1;
     }
 
+    // Autotuner results per (device, precision, grid): the y/z passes do not
+    // depend on the particles, so later configurations of the same shape reuse
+    // the choice (the analogue of FFTW wisdom across configurations).
+    struct Tuned {
+        int ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk;
+    };
+    static std::mutex& tune_mu() {
+        static std::mutex m;
+        return m;
+    }
+    static std::map<std::array<int, 5>, Tuned>& tune_cache() {
+        static std::map<std::array<int, 5>, Tuned> c;
+        return c;
+    }
+
     int autotune() {
         const bool verbose = std::getenv("FFCM_VERBOSE") != nullptr;
         int fyk, fyB, fzk, fzB;
         forced_variant("FFCM_FORCE_Y", fyk, fyB);
         forced_variant("FFCM_FORCE_Z", fzk, fzB);
+        const bool forced = fyk >= 0 || fzk >= 0 || std::getenv("FFCM_FORCE_CHUNK") != nullptr;
+        int dev = 0;
+        CUDA_TRY(cudaGetDevice(&dev));
+        const std::array<int, 5> key{dev, (int)sizeof(T), Mx, My, Mz};
+        if (!forced) {
+            std::lock_guard<std::mutex> lock(tune_mu());
+            auto it = tune_cache().find(key);
+            if (it != tune_cache().end()) {
+                const Tuned& t = it->second;
+                const bool maps_ok = (t.ykind != 2 || ymap_ok[log2i(t.By)]) && (t.zkind != 3 || zmap_ok[log2i(t.Bz)]);
+                if (maps_ok) {
+                    ykind = t.ykind; By = t.By; ygrid = t.ygrid;
+                    zkind = t.zkind; Bz = t.Bz; zgrid = t.zgrid;
+                    kx_chunk = t.kx_chunk;
+                    if (verbose) fprintf(stderr, "ffcm autotune: reusing the choice for %dx%dx%d\n", Mx, My, Mz);
+                    return FFCM_OK;
+                }
+            }
+        }
         if (fast_y) {
             float best = 1e30f;
             int bk = 0, bB = By, bg = 0;
@@ -788,6 +831,10 @@ struct Engine final : EngineBase {
         }
         CUDA_TRY(cudaStreamSynchronize(h->stream));
         h->launches = 0;
+        if (!forced) {
+            std::lock_guard<std::mutex> lock(tune_mu());
+            tune_cache()[key] = Tuned{ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk};
+        }
         return FFCM_OK;
     }
     int tuned_By = 0, tuned_Bz = 0;
@@ -894,6 +941,12 @@ struct Engine final : EngineBase {
 
     int mobility_rest(void* V, cudaStream_t s) override { return solve(V, s, false); }
     int mobility_rest_same_positions(void* V, cudaStream_t s) override { return solve(V, s, false, false); }
+    int apply_fixed(void* V, const void* F, cudaStream_t s) override {
+        TRY(gather_forces(F, s));
+        TRY(solve(V, s, false, !lists_built));
+        lists_built = true;
+        return FFCM_OK;
+    }
 
     // keep_u: also leave the velocity grid u = L^-1 S F in gu (the adjoint's
     // only checkpoint); the unfused pipeline leaves it there anyway.
@@ -1280,6 +1333,7 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
     g_err.clear();
     TRY(check_handle(h));
     h->ckpt = false;
+    h->positions = false;
     TRY(check_memory(memory));
     const int64_t N = h->N;
     if (!(vr == 3 && vc == N && yr == 3 && yc == N && fr == 3 && fc == N)) {
@@ -1322,6 +1376,7 @@ int ffcm_wrap_positions(ffcm_handle* h, const void* Y, int32_t memory, void* str
     g_err.clear();
     TRY(check_handle(h));
     h->ckpt = false;
+    h->positions = false;
     TRY(check_memory(memory));
     if (!Y) return fail(FFCM_ERR_ARGUMENT, "Y must not be NULL");
     DeviceGuard g(h->device);
@@ -1340,6 +1395,7 @@ int ffcm_assign_cells(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
     h->ckpt = false;
+    h->positions = false;
     DeviceGuard g(h->device);
     return h->eng->wrap_hash(nullptr, false, true, h->pick(stream));
 }
@@ -1348,6 +1404,7 @@ int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, v
     g_err.clear();
     TRY(check_handle(h));
     h->ckpt = false;
+    h->positions = false;
     TRY(check_memory(memory));
     if (!F) return fail(FFCM_ERR_ARGUMENT, "F must not be NULL");
     DeviceGuard g(h->device);
@@ -1366,6 +1423,7 @@ int ffcm_spread_forces(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
     h->ckpt = false;
+    h->positions = false;
     DeviceGuard g(h->device);
     return h->eng->spread(h->pick(stream));
 }
@@ -1374,6 +1432,7 @@ int ffcm_stokes_solve(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
     h->ckpt = false;
+    h->positions = false;
     DeviceGuard g(h->device);
     return h->eng->stokes(h->pick(stream));
 }
@@ -1413,6 +1472,7 @@ int ffcm_mobility_checkpoint(ffcm_handle* h, void* V, const void* Y, const void*
     TRY(check_handle(h));
     TRY(check_memory(memory));
     h->ckpt = false;
+    h->positions = false;
     if (!V || !Y || !F) return fail(FFCM_ERR_ARGUMENT, "V, Y and F must not be NULL");
     DeviceGuard g(h->device);
     cudaStream_t s = h->pick(stream);
@@ -1479,6 +1539,7 @@ int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, v
     TRY(check_handle(h));
     TRY(check_memory(memory));
     h->ckpt = false;
+    h->positions = false;
     if (!J || !dJdY || !dJdF || !V || !Y || !F || !V_target)
         return fail(FFCM_ERR_ARGUMENT, "no argument of ffcm_objective_gradient may be NULL");
     DeviceGuard g(h->device);
@@ -1520,6 +1581,66 @@ int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, v
         return rc;
     }
     CUDA_TRY(cudaMemcpyAsync(J, Jdev, sizeof(double), cudaMemcpyDeviceToDevice, s));
+    return FFCM_OK;
+}
+
+int ffcm_set_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    TRY(check_memory(memory));
+    h->ckpt = false;
+    h->positions = false;
+    if (!Y) return fail(FFCM_ERR_ARGUMENT, "Y must not be NULL");
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    const void* Yd = Y;
+    if (memory == FFCM_HOST) {
+        StageScope sc(h, FFCM_STAGE_H2D, s);
+        CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));
+        Yd = e->Y_in();
+    }
+    // the sort gathers some forces along; zeros stand in until the first apply
+    CUDA_TRY(cudaMemsetAsync(e->F_in(), 0, bytes, s));
+    TRY(e->wrap_hash(Yd, true, true, s));
+    TRY(e->sort(e->F_in(), s));
+    e->lists_built = false;
+    if (memory == FFCM_HOST) TRY(finish(h, s));
+    h->positions = true;
+    return FFCM_OK;
+}
+
+int ffcm_mobility_apply(ffcm_handle* h, void* V, const void* F, int32_t memory, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    TRY(check_memory(memory));
+    if (!V || !F) return fail(FFCM_ERR_ARGUMENT, "V and F must not be NULL");
+    if (!h->positions)
+        return fail(FFCM_ERR_STATE,
+                    "ffcm_mobility_apply needs the cell list of a preceding ffcm_set_positions on this handle, "
+                    "with no other solve or step call in between");
+    h->ckpt = false;
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    const void* Fd = F;
+    void* Vd = V;
+    if (memory == FFCM_HOST) {
+        StageScope sc(h, FFCM_STAGE_H2D, s);
+        CUDA_TRY(cudaMemcpyAsync(e->F_in(), F, bytes, cudaMemcpyHostToDevice, s));
+        Fd = e->F_in();
+        Vd = e->V_out();
+    }
+    TRY(e->apply_fixed(Vd, Fd, s));
+    if (memory == FFCM_HOST) {
+        {
+            StageScope sc(h, FFCM_STAGE_D2H, s);
+            CUDA_TRY(cudaMemcpyAsync(V, e->V_out(), bytes, cudaMemcpyDeviceToHost, s));
+        }
+        return finish(h, s);
+    }
     return FFCM_OK;
 }
 
@@ -1658,13 +1779,16 @@ int ffcm_get_buffer(ffcm_handle* h, int32_t which, void* dst, int64_t nbytes, in
 
 int ffcm_set_buffer(ffcm_handle* h, int32_t which, const void* src, int64_t nbytes,
                     int32_t memory, void* stream) {
+    if (h) {   // the overwritten state no longer matches a checkpoint or cached cell list
+        h->ckpt = false;
+        h->positions = false;
+    }
     return buffer_dispatch(h, which, const_cast<void*>(src), nbytes, memory, stream, false);
 }
 
 int ffcm_synchronize(ffcm_handle* h, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    h->ckpt = false;
     DeviceGuard g(h->device);
     return finish(h, h->pick(stream));
 }

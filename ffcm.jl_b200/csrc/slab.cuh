@@ -242,6 +242,15 @@ struct SpreadWin {
     int scan[32];
 };
 
+// Bytes of the spread window region: the window, or the idle-lane FFT line
+// that aliases it, whichever is larger (16-byte multiple).
+template <typename T, int BY, int BZ, int H>
+__host__ __device__ constexpr size_t spread_win_bytes() {
+    return ((sizeof(SpreadWin<T, BY, BZ, H>) > (size_t)padded_len(H) * sizeof(cplx<T>)
+                 ? sizeof(SpreadWin<T, BY, BZ, H>)
+                 : (size_t)padded_len(H) * sizeof(cplx<T>)) + 15) / 16 * 16;
+}
+
 template <typename T, int BY, int BZ, int H>
 __device__ __forceinline__ void spread_put(const StencilParams<T>& p, SpreadWin<T, BY, BZ, H>& W, int i,
                                            const vec4<T>& y, const vec4<T>& f, int sx, int sy, int sz,
@@ -278,7 +287,9 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
     SpreadWin<T, BY, BZ, H>& W = *reinterpret_cast<SpreadWin<T, BY, BZ, H>*>(acc + ROWS * P);
     // exchange line of idle FFT lanes: the window is dead by then
     cplx<T>* dummy = reinterpret_cast<cplx<T>*>(&W);
-    const cplx<T>* tw = twx;   // twiddles are read through L1
+    // FFT twiddles in shared memory, after the window / idle-lane line
+    cplx<T>* tw = reinterpret_cast<cplx<T>*>(reinterpret_cast<unsigned char*>(&W) + spread_win_bytes<T, BY, BZ, H>());
+    load_table(tw, twx, Mx);
     const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
     for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
@@ -478,7 +489,8 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
     __shared__ __align__(8) uint64_t bar;
     T* acc = reinterpret_cast<T*>(smem_raw);
     cplx<T>* dummy = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
-    const cplx<T>* tw = twx;   // twiddles are read through L1
+    cplx<T>* tw = dummy + padded_len(H);   // FFT twiddles in shared memory
+    load_table(tw, twx, Mx);
     const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
     // all of the slab's spectrum rows arrive in one batch of bulk copies
@@ -623,8 +635,9 @@ SlabKernels<T> slab_kernels_for() {
     k.BZ = BZ;
     const size_t slab_bytes = (size_t)3 * BY * BZ * slab_pitch(2 * H) * sizeof(T);
     const size_t line_bytes = (size_t)padded_len(H) * sizeof(cplx<T>);
-    k.smem = slab_bytes + std::max(sizeof(SpreadWin<T, BY, BZ, H>), line_bytes);
-    k.smem_interp = slab_bytes + line_bytes;
+    const size_t table_bytes = (size_t)2 * H * sizeof(cplx<T>);
+    k.smem = slab_bytes + spread_win_bytes<T, BY, BZ, H>() + table_bytes;
+    k.smem_interp = slab_bytes + line_bytes + table_bytes;
     return k;
 }
 

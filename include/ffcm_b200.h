@@ -170,6 +170,18 @@ int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* s
  * (src/correct_velocities.jl:154-286). V is 3xN. */
 int ffcm_correct_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream);
 
+/* ---- fixed-position operator ----------------------------------------------
+ * FFCMMobility(config, Y) applied many times (src/mobility.jl:374-448): the
+ * positions are wrapped, hashed and sorted once; every apply re-gathers the
+ * forces into that order and solves. The results equal ffcm_mobility's. */
+
+/* Fix the positions (Julia 3xN Y) for the following applies. */
+int ffcm_set_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stream);
+/* V = M(Y) F for the positions of the last ffcm_set_positions; replaces
+ * mul!(v, M, f) / M * F. FFCM_ERR_STATE if any other solve or step call ran
+ * on the handle since. */
+int ffcm_mobility_apply(ffcm_handle* h, void* V, const void* F, int32_t memory, void* stream);
+
 /* ---- buffer access (step isolation, as test/cuda/ does) ------------------ */
 int64_t ffcm_buffer_bytes(const ffcm_handle* h, int32_t which);
 int ffcm_get_buffer(ffcm_handle* h, int32_t which, void* dst, int64_t nbytes, int32_t memory,

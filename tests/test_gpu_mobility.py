@@ -292,3 +292,33 @@ def test_configurations_of_different_sizes_alive_at_once(ffcm):
         ffcm.mobility(V, cfg, Y, F)
         ora = O.OracleConfig(np.float64, **kw_of(L, cfg.N, cfg.num_grid_points[0], R_c=3.0))
         assert rel_l2(V, O.apply(ora, Y, F)) < 1e-10
+
+
+@pytest.mark.parametrize("T", TS)
+def test_fixed_position_operator(ffcm, T):
+    """FFCMMobility fixes the positions once (ffcm_set_positions) and applies
+    with re-gathered forces (ffcm_mobility_apply): each application equals the
+    plain solve, also after another solve on the same configuration."""
+    N, L, M = 2000, 40.0, 64
+    rng = np.random.default_rng(31)
+    Y = nonoverlapping_uniform(N, L, 5).astype(T)
+    cfg = ffcm.FFCMConfig(T, **kw_of(L, N, M, R_c=3.0))
+    lib = ffcm._lib.load()
+    V = np.empty((N, 3), T)
+    F0 = rng.standard_normal((N, 3)).astype(T)
+    assert lib.ffcm_mobility_apply(cfg.handle, V.ctypes.data, F0.ctypes.data, 0, None) == ffcm._lib.ERR_STATE
+    Mop = ffcm.FFCMMobility(cfg, Y)
+    tol = 1e-6 if T == np.float32 else 1e-12
+    for k in range(3):
+        F = rng.standard_normal((N, 3)).astype(T)
+        Vp = np.empty_like(Y)
+        Va = Mop @ F
+        ffcm.mobility(Vp, cfg, Y, F)          # a plain solve in between invalidates the cache
+        assert rel_l2(Va, Vp) < tol
+    Y2 = nonoverlapping_uniform(N, L, 6).astype(T)
+    Vo = np.empty_like(Y)
+    ffcm.mobility(Vo, cfg, Y2, F0)            # other positions on the same config
+    Va = Mop @ F0                             # the operator re-fixes its own positions
+    Vp = np.empty_like(Y)
+    ffcm.mobility(Vp, cfg, Y, F0)
+    assert rel_l2(Va, Vp) < tol
