@@ -62,7 +62,7 @@ def random_cloud(T, N, L, seed):
     return Y, F
 
 
-def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None, draw=None, max_phi=0.3):
+def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None, max_phi=0.3):
     """Uniform i.i.d. positions in the box [0, L)^3 (L a scalar or a 3-tuple),
     rejection-sampled so that no two centres are closer than `min_sep` (2a for
     unit spheres).
@@ -72,9 +72,6 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None, draw=None, max_p
     (both members of a conflicting in-batch pair are dropped). Neighbour checks
     use a periodic cell grid of side >= min_sep, so the cost is O(N). Returns
     float64 positions of shape (N, 3) in random (shuffled) order.
-
-    `draw(rng, B, last_acceptance)` replaces the uniform candidate draw (it
-    returns B positions in the box); `clustered_nonoverlapping` uses it.
     """
     rng = np.random.default_rng(seed)
     L = np.broadcast_to(np.asarray(L, np.float64), (3,)).copy()
@@ -92,13 +89,12 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None, draw=None, max_p
     offs = np.array([(dx, dy, dz) for dx in (-1, 0, 1) for dy in (-1, 0, 1) for dz in (-1, 0, 1)])
     ms2 = min_sep * min_sep
     stalled = 0
-    last_rate = 1.0
     while count < N:
         if stalled > 200:
             raise RuntimeError(f"placed {count} of {N} spheres; no progress in 200 batches")
         need = N - count
         B = batch or max(1024, int(need * 1.3))
-        cand = rng.random((B, 3)) * L if draw is None else draw(rng, B, last_rate)
+        cand = rng.random((B, 3)) * L
         cc = np.minimum((cand / cs).astype(np.int64), ncv - 1)
         ok = np.ones(B, bool)
         # against kept centres
@@ -157,47 +153,25 @@ def nonoverlapping_uniform(N, L, seed, min_sep=2.0, batch=None, draw=None, max_p
             pos[count:count + acc.size] = cand[acc]
             count += acc.size
         stalled = 0 if acc.size else stalled + 1
-        last_rate = acc.size / B
     perm = rng.permutation(N)
     return pos[perm]
 
 
-def clustered_nonoverlapping(N, L, nclusters, seed, log_mean=float(np.log(3.0)), log_sigma=0.5,
-                             min_sep=2.0):
-    """Non-overlapping spheres in Gaussian clusters: cluster centres uniform in
-    the cubic box, per-cluster standard deviation log-normal(log_mean,
-    log_sigma), each candidate drawn from a uniformly chosen cluster and
-    rejection-tested as in `nonoverlapping_uniform`.
+def clustered_gaussian(N, L, nclusters, seed, log_mean=float(np.log(3.0)), log_sigma=0.5):
+    """Positions in Gaussian clusters: centres uniform in the cubic box [0, L)^3,
+    per-cluster standard deviation log-normal(log_mean, log_sigma), each
+    sphere in a uniformly chosen cluster, wrapped into the box.
 
-    At high volume fractions the cluster cores jam (random sequential addition
-    stops near 38%), so once fewer than 5% of a batch of cluster candidates
-    are accepted, or after 10 clustered batches, the remaining spheres are
-    drawn uniformly. Returns the positions and the coefficient of variation
-    of the particle counts of cells of side 4 (about 0.25 for the uniform
-    placement at 10%; larger means clustered).
+    No non-overlap test: at the clustered workload's 31% volume fraction,
+    rejection sampling jams the cluster cores after a few batches and the
+    result is indistinguishable from a uniform placement, so the spheres of a
+    cluster may overlap (the method is defined for any distinct positions).
     """
-    rng0 = np.random.default_rng(seed + 7919)
-    centres = rng0.random((nclusters, 3)) * L
-    widths = np.exp(rng0.normal(log_mean, log_sigma, nclusters))
-    state = {"uniform": False, "clustered_batches": []}
-
-    def draw(rng, B, last_rate):
-        nb = len(state["clustered_batches"])
-        if not state["uniform"] and nb and (last_rate < 0.05 or nb >= 10):
-            state["uniform"] = True
-        if state["uniform"]:
-            state["clustered_batches"].append(False)
-            return rng.random((B, 3)) * L
-        state["clustered_batches"].append(True)
-        c = rng.integers(nclusters, size=B)
-        return (centres[c] + rng.standard_normal((B, 3)) * widths[c, None]) % L
-
-    # the uniform stage needs the whole box; 0.33 stays below jamming
-    Y = nonoverlapping_uniform(N, L, seed, min_sep=min_sep, draw=draw, max_phi=0.33)
-    nc = max(1, int(L // 4.0))
-    counts = np.bincount(np.ravel_multi_index(np.minimum((Y / (L / nc)).astype(np.int64), nc - 1).T,
-                                              (nc, nc, nc)), minlength=nc ** 3)
-    return Y, float(counts.std() / counts.mean())
+    rng = np.random.default_rng(seed)
+    centres = rng.random((nclusters, 3)) * L
+    widths = np.exp(rng.normal(log_mean, log_sigma, nclusters))
+    c = rng.integers(nclusters, size=N)
+    return (centres[c] + rng.standard_normal((N, 3)) * widths[c, None]) % L
 
 
 def box_for_volume_fraction(N, phi, a=1.0):

@@ -322,3 +322,21 @@ def test_fixed_position_operator(ffcm, T):
     Vp = np.empty_like(Y)
     ffcm.mobility(Vp, cfg, Y, F0)
     assert rel_l2(Va, Vp) < tol
+
+
+@pytest.mark.parametrize("T", TS)
+def test_clustered_suspension_matches_oracle(ffcm, T):
+    """Gaussian clusters at the clustered workload's density (31% by volume,
+    overlaps allowed), 256^3: dense slabs overflow their particle lists and
+    take the slab kernels' own candidate scan; the result still equals the
+    oracle's."""
+    from fixtures import clustered_gaussian
+    N, L, M = 31_250, 75.0, 256
+    Y = clustered_gaussian(N, L, 250, 2029).astype(T)
+    F = np.random.default_rng(3).standard_normal((N, 3)).astype(T)
+    kw = kw_of(L, N, M, R_c=3.0)
+    prod, ora = both(ffcm, T, **kw)
+    V = np.empty_like(Y)
+    ffcm.mobility(V, prod, Y, F)
+    err = rel_l2(V, O.apply(ora, Y, F))
+    assert err < (1e-5 if T == np.float32 else 1e-10), err
