@@ -218,7 +218,7 @@ template <typename T>
 ZTmaKernel<T> ztma_kernel(int n, int B) {
 #define FFCM_ZT(NN, BB) if (n == NN && B == BB) return k_fftt_z_stokes<T, NN, BB>;
     FFCM_ZT(64, 8) FFCM_ZT(64, 16) FFCM_ZT(128, 4) FFCM_ZT(128, 8) FFCM_ZT(256, 2) FFCM_ZT(256, 4)
-    FFCM_ZT(512, 2) FFCM_ZT(512, 4) FFCM_ZT(512, 8) FFCM_ZT(1024, 2)
+    FFCM_ZT(512, 2) FFCM_ZT(512, 4) FFCM_ZT(512, 8) FFCM_ZT(1024, 2) FFCM_ZT(1024, 4)
 #undef FFCM_ZT
     return nullptr;
 }

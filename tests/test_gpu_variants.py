@@ -17,7 +17,12 @@ pytestmark = pytest.mark.gpu
 
 CASES = {"64^3": dict(L=(40.0,) * 3, N=2000, M=(64, 64, 64)),
          "128^3": dict(L=(60.0,) * 3, N=5000, M=(128, 128, 128)),
-         "64x32x32": dict(L=(32.0, 16.0, 16.0), N=300, M=(64, 32, 32))}
+         "64x32x32": dict(L=(32.0, 16.0, 16.0), N=300, M=(64, 32, 32)),
+         # lines of 1024 along z, y and x (the last through the slab kernels at
+         # x length 1024), spacing and density of the 64^3 case
+         "64x64x1024": dict(L=(40.0, 40.0, 640.0), N=32000, M=(64, 64, 1024)),
+         "64x1024x64": dict(L=(40.0, 640.0, 40.0), N=32000, M=(64, 1024, 64)),
+         "1024x64x64": dict(L=(640.0, 40.0, 40.0), N=32000, M=(1024, 64, 64))}
 Y_VARIANTS = [(k, B) for k in (0, 1, 2) for B in (2, 4, 8, 16)]
 Z_VARIANTS = [(k, B) for k in (0, 1, 2, 3) for B in (2, 4, 8, 16)]
 
