@@ -215,6 +215,19 @@ def run_reference(args, rank, world):
         config = adjoint_config()
         sample = (f"{warm} warm-up + {steps} timed objective-gradient evaluations of the workload by "
                   "the C/pocketfft restatement (forward, residual, pullback)")
+    elif args.workload == "resistance":
+        Y, V = resistance_inputs()
+        cfg = O.OracleConfig(np.float32, **config_kwargs(), fft_threads=threads)
+
+        def fn():
+            t0 = time.perf_counter()
+            O.cg(cfg, Y, V, maxiter=1)
+            return time.perf_counter() - t0
+
+        units, unit, metric, config = Y.shape[0], "particles/s", RES_METRIC, resistance_config()
+        sample = (f"{warm} warm-up + {steps} timed CG iterations (maxiter = 1: one operator application "
+                  "and the vector updates) of the workload by the C/pocketfft restatement; "
+                  "particles/s per CG iteration of that sample")
     elif args.workload == "batched":
         from fixtures import nonoverlapping_uniform
         b = BATCH
@@ -828,6 +841,150 @@ def run_clustered(args, rank, world, local_rank):
     return 0
 
 
+RES_METRIC = ("particles/s per CG iteration of the resistance solve M(Y) F = V "
+              "(N=500k, 512^3, Float32, to |r| <= sqrt(eps) |V|)")
+
+
+def resistance_config():
+    c = workload_config()
+    c["workload"] = ("resistance solve M(Y) F = V by conjugate gradients on the mobility operator "
+                     "(IterativeSolvers cg stopping rule, reltol = sqrt(eps(Float32)), F0 = 0); "
+                     + c["workload"].replace("plain FFCM mobility, ", ""))
+    return c
+
+
+def resistance_inputs():
+    Y, _ = make_inputs()
+    V = np.random.default_rng(WORK["seed"] + 7).standard_normal(Y.shape).astype(np.float32)
+    return Y, V
+
+
+def run_resistance(args, rank, world, local_rank):
+    import torch
+    ffcm = _load_product()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    Y, V = resistance_inputs()
+    N = Y.shape[0]
+    cfg = ffcm.FFCMConfig(np.float32, device=local_rank, **config_kwargs())
+    Yd, Vd = torch.from_numpy(Y).to(dev), torch.from_numpy(V).to(dev)
+    Fd = torch.empty_like(Yd)
+    stream = torch.cuda.current_stream(dev)
+    op = ffcm.FFCMMobility(cfg, Yd)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize(dev)
+
+    def timed(fn, steps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
+    hist = []
+
+    def solve():
+        # positions fixed (wrap, hash, sort) and the whole CG loop: one resistance solve
+        op._set_positions()
+        hist.append(ffcm.cg(op, Vd, out=Fd, log=True)[1])
+
+    for _ in range(args.warmup):
+        solve()
+    launches0 = cfg.launch_count()
+    hist.clear()
+    with ClockSampler(local_rank) as clk:
+        ms = timed(solve, args.steps)
+    launches = cfg.launch_count() - launches0
+    iters = hist[-1].iters
+    assert all(h.iters == iters for h in hist) and hist[-1].isconverged
+    # one operator application alone (the iteration's dominant part)
+    lib = ffcm.L_.load()
+    sh = ffcm._stream_handle(stream)
+    W = torch.empty_like(Yd)
+    ms_apply = timed(lambda: lib.ffcm_mobility_apply(cfg.handle, W.data_ptr(), Fd.data_ptr(), 1, sh), args.steps)
+    cfg.profile_begin()
+    lib.ffcm_mobility_apply(cfg.handle, W.data_ptr(), Fd.data_ptr(), 1, sh)
+    torch.cuda.synchronize(dev)
+    stages = cfg.profile_end()
+    # end to end: host Y and V in, F out, every step
+    Yh, Vh = torch.from_numpy(Y).pin_memory(), torch.from_numpy(V).pin_memory()
+    Fh = torch.empty_like(Yh).pin_memory()
+
+    def solve_host():
+        o = ffcm.FFCMMobility(cfg, Yh)
+        ffcm.cg(o, Vh, out=Fh)
+
+    solve_host()
+    ms_e2e = timed(solve_host, args.steps)
+    if dist is not None:
+        t = torch.tensor([ms, ms_apply, ms_e2e], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_apply, ms_e2e = (float(x) for x in t)
+    if rank == 0:
+        per, solve_bytes = algorithmic_bytes()
+        peak, peak_kind = measured_peak_hbm()
+        stage_ms = {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1] > 0}
+        ks = [k for k in per if k in stage_ms]
+        dom = max(ks, key=lambda k: stage_ms[k])
+        achieved = per[dom] / (stage_ms[dom] / 1e3) / 1e9
+        # per iteration: one application without the cell list, plus the CG
+        # vector kernels (direction: 2 reads 1 write; alpha: 2 reads; update: 4 reads 2 writes)
+        it_bytes = solve_bytes - per["cell_list"] + 11 * 3 * N * 4
+        ms_iter = ms / max(iters, 1)
+        cpu = None
+        if not args.skip_cpu_baseline:
+            import ffcm_oracle as O
+            threads = os.cpu_count() or 1
+            ocfg = O.OracleConfig(np.float32, **config_kwargs(), fft_threads=threads)
+            t0 = time.perf_counter()
+            O.cg(ocfg, Y, V, maxiter=1)
+            sec = time.perf_counter() - t0
+            cpu = {"value": N / sec, "unit": "particles/s", "cores": threads, "kind": "port",
+                   "sample": "one CG iteration (one operator application + vector updates) of the "
+                             "workload by the C/pocketfft oracle"}
+        line = {
+            "metric": RES_METRIC, "value": world * N * iters / (ms / 1e3), "unit": "particles/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {**resistance_config(), "parallelism": "replicas" if world > 1 else "single"},
+            "iterations": iters, "resnorm_rel": hist[-1].resnorm / float(np.linalg.norm(V.astype(np.float64))),
+            "solves_per_s": world * 1e3 / ms, "ms_per_iteration": ms_iter, "apply_ms": ms_apply,
+            "cg_overhead_per_iteration_ms": ms_iter - ms_apply,
+            "e2e": {"value": world * N * iters / (ms_e2e / 1e3), "unit": "particles/s", "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": int(Yh.numel() * 4 + Vh.numel() * 4),
+                    "d2h_bytes_per_step": int(Fh.numel() * 4)},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": ncu_traffic(dom),
+                         "algorithmic_bytes_per_launch": per[dom]},
+            "iteration_roofline": {"algorithmic_bytes": it_bytes,
+                                   "achieved_GBs": it_bytes / (ms_iter / 1e3) / 1e9,
+                                   "frac": it_bytes / (ms_iter / 1e3) / 1e9 / peak},
+            "apply_stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    cfg.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def cpu_adjoint_run(Y, F, Vt, threads):
     import ffcm_oracle as O
     cfg = O.OracleConfig(np.float32, **adjoint_kwargs(), fft_threads=threads)
@@ -856,7 +1013,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["plain", "batched", "adjoint", "clustered"], default="plain")
+    ap.add_argument("--workload", choices=["plain", "batched", "adjoint", "clustered", "resistance"], default="plain")
     ap.add_argument("--grid", default=None,
                     help="Mx,My,Mz: smaller case at the same spacing and density (profiling)")
     args = ap.parse_args()
@@ -876,6 +1033,8 @@ def main():
         return run_adjoint(args, rank, world, local_rank)
     if args.workload == "clustered":
         return run_clustered(args, rank, world, local_rank)
+    if args.workload == "resistance":
+        return run_resistance(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -36,7 +36,7 @@ __all__ = ["FFCMConfig", "mobility", "FFCMMobility", "FFCMBatch", "ArgumentError
            "FFCMError", "wrap_positions", "assign_cells", "sort_particles_by_cell",
            "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities",
            "mobility_checkpoint", "adjoint", "objective_gradient", "rrule_mobility",
-           "mobility_autograd"]
+           "mobility_autograd", "cg", "CGHistory"]
 
 
 class ArgumentError(ValueError):
@@ -381,7 +381,8 @@ class FFCMMobility:
     """
 
     def __init__(self, config: FFCMConfig, Y):
-        Y = np.asarray(Y)
+        if not _is_torch(Y):
+            Y = np.asarray(Y)
         r, c = _julia_size(Y)
         if r != 3:
             raise ArgumentError(f"Y must be 3xN; got size ({r}, {c})")
@@ -389,13 +390,18 @@ class FFCMMobility:
             raise ArgumentError(f"Y has {c} particles but config was built for {config.N}; "
                                 "construct a config with matching N")
         self.config = config
-        self.Y = np.ascontiguousarray(Y, config.T).copy()
+        if _is_torch(Y):
+            # a CUDA tensor stays on the device (a private copy: Y is never mutated)
+            self.Y = _Arg(Y, config.T).buf.detach().clone()
+        else:
+            self.Y = np.ascontiguousarray(Y, config.T).copy()
         self.F_scratch = np.empty((config.N, 3), config.T)
         self.V_scratch = np.empty((config.N, 3), config.T)
         self._set_positions()
 
     def _set_positions(self):
-        _raise(L_.load().ffcm_set_positions(self.config.handle, self.Y.ctypes.data, L_.HOST, None))
+        y = _Arg(self.Y, self.config.T)
+        _raise(L_.load().ffcm_set_positions(self.config.handle, y.ptr, y.memory, _stream_of(y)))
 
     def _apply(self, V, F):
         """V = M F for (N, 3) host arrays of the config's type."""
@@ -454,6 +460,71 @@ class FFCMMobility:
     @staticmethod
     def isposdef():
         return True
+
+
+# ---- resistance problem: conjugate gradients on the operator ----
+
+class CGHistory:
+    """What ``cg(...; log=true)`` of IterativeSolvers.jl reports and a caller
+    reads: ``isconverged``, ``iters`` (iterations, one operator application
+    each), ``resnorm`` (|r| of the recursion at the end) and ``status``
+    ('converged', 'maxiter' or 'breakdown')."""
+
+    def __init__(self, iters, resnorm, status):
+        self.iters = int(iters)
+        self.resnorm = float(resnorm)
+        self.status = L_.CG_STATUS.get(int(status), f"status {int(status)}")
+        self.isconverged = self.status == "converged"
+
+    def __repr__(self):
+        return f"CGHistory(iters={self.iters}, resnorm={self.resnorm:.3e}, status={self.status!r})"
+
+
+def cg(M: FFCMMobility, V, *, reltol=None, abstol=0.0, maxiter=None, log=False, x0=None, out=None,
+       stream=None):
+    """Solve the resistance problem M(Y) F = V for F by conjugate gradients,
+    the use the reference declares ``FFCMMobility`` symmetric positive definite
+    for (src/mobility.jl:161-162; ``cg(M, V)`` of IterativeSolvers.jl in
+    Julia). The whole iteration runs on the device (``ffcm_cg_solve``).
+
+    Keywords as IterativeSolvers.jl's ``cg``: stop once
+    |r| <= max(reltol |r0|, abstol) or after ``maxiter`` iterations;
+    ``reltol`` defaults to sqrt(eps(T)), ``maxiter`` to 3N. ``x0`` is an
+    initial guess (default zero, ``initially_zero``). ``V`` (and ``out``,
+    ``x0``) are 3xN host arrays or all CUDA tensors of the config's type.
+    Returns F, or ``(F, CGHistory)`` with ``log=True``.
+    """
+    config = M.config
+    T = config.T
+    if out is None:
+        if _is_torch(V):
+            import torch
+            out = torch.empty_like(V)
+        else:
+            out = np.empty((config.N, 3), T)
+    flags = 0
+    if x0 is not None:
+        out[...] = x0 if _is_torch(out) else np.asarray(x0, T).reshape(config.N, 3)
+        flags = L_.CG_INITIAL_GUESS
+    f, v = _particle_args(config, (("F", out), ("V", V)), writable=("F",))
+    st = _stream_of(f) if stream is None else _stream_handle(stream)
+    it, res, status = ctypes.c_int32(0), ctypes.c_double(0.0), ctypes.c_int32(0)
+    rt = -1.0 if reltol is None else float(reltol)
+    mi = -1 if maxiter is None else int(maxiter)
+    lib = L_.load()
+
+    def call():
+        return lib.ffcm_cg_solve(config.handle, f.ptr, v.ptr, f.memory, rt, float(abstol), mi, flags,
+                                 ctypes.byref(it), ctypes.byref(res), ctypes.byref(status), st)
+
+    code = call()
+    if code == L_.ERR_STATE:     # the config solved something else since
+        M._set_positions()
+        code = call()
+    _raise(code)
+    if log:
+        return out, CGHistory(it.value, res.value, status.value)
+    return out
 
 
 # ---- adjoint form (no reference counterpart: the reference has no derivative) ----

@@ -27,6 +27,10 @@ ERR_STATE = 7
 
 FLOAT32 = 0
 FLOAT64 = 1
+
+# conjugate gradients (ffcm_cg_solve)
+CG_INITIAL_GUESS = 1
+CG_STATUS = {1: "converged", 2: "maxiter", 3: "breakdown"}
 HOST = 0
 DEVICE = 1
 
@@ -85,6 +89,8 @@ SIGNATURES = {
     "ffcm_sort_cells_noalloc": (_c.c_int, [_vp, _i64, _i32, _vp, _vp, _vp, _vp]),
     "ffcm_set_positions": (_c.c_int, [_vp, _vp, _i32, _vp]),
     "ffcm_mobility_apply": (_c.c_int, [_vp, _vp, _vp, _i32, _vp]),
+    "ffcm_cg_solve": (_c.c_int, [_vp, _vp, _vp, _i32, _c.c_double, _c.c_double, _i32, _i32, _vp, _vp, _vp,
+                                 _vp]),
 }
 
 _lib = None

@@ -20,6 +20,7 @@
 #include "cell_list.cuh"
 #include "correct.cuh"
 #include "adjoint.cuh"
+#include "cg.cuh"
 #include "fft.cuh"
 #include "fft_dispatch.cuh"
 #include "fft_pipe.cuh"
@@ -250,6 +251,15 @@ struct EngineBase {
     virtual void* Y_in() = 0;
     virtual void* F_in() = 0;
     virtual void* V_out() = 0;
+    // conjugate gradients on apply_fixed (the resistance problem): the slab
+    // particle lists (or the real grids of the generic pipeline) made ready
+    // outside any graph capture; r = V - q, p = 0 and the scalar state; one
+    // iteration (p update, q = M p, alpha, x/r update and the loop condition)
+    virtual int ensure_lists(cudaStream_t s) = 0;
+    virtual int cg_start(const void* V, const void* q, void* r, void* p, CgState* st, double reltol,
+                         double abstol, int maxiter, cudaStream_t s) = 0;
+    virtual int cg_iteration(void* x, void* r, void* p, void* q, CgState* st, cudaGraphConditionalHandle loop,
+                             cudaStream_t s) = 0;
 };
 
 }  // namespace
@@ -279,6 +289,23 @@ struct ffcm_handle {
     size_t next_event = 0;
     std::vector<std::pair<int, size_t>> recorded;  // (stage, index of the start event)
     std::unique_ptr<EngineBase> eng;
+    // conjugate-gradient solver state (allocated by the first ffcm_cg_solve):
+    // solution, residual, direction and product vectors (3N each), the
+    // device scalar state and its pinned host copy, and the graph of the
+    // iteration loop on its own capture stream
+    struct Cg {
+        void* x = nullptr;
+        void* r = nullptr;
+        void* p = nullptr;
+        void* q = nullptr;
+        CgState* st = nullptr;
+        CgState* host = nullptr;
+        cudaStream_t cs = nullptr;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        cudaGraphConditionalHandle loop = 0;
+        int64_t body_kernels = 0;  // kernels per iteration
+    } cg;
     // host copies of derived data for get_buffer
     std::vector<double> kx, ky, kz;
 
@@ -948,6 +975,39 @@ struct Engine final : EngineBase {
         return FFCM_OK;
     }
 
+    int ensure_lists(cudaStream_t s) override {
+        if (lists_built) return FFCM_OK;
+        if (slab) {
+            StageScope sc(h, FFCM_STAGE_SPREAD, s);
+            const int nslab = sg.nty * sg.ntz;
+            TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
+                       slab_lists, slab_counts));
+        } else {
+            TRY(ensure_real_grids());
+        }
+        lists_built = true;
+        return FFCM_OK;
+    }
+
+    int cg_start(const void* V, const void* q, void* r, void* p, CgState* st, double reltol, double abstol,
+                 int maxiter, cudaStream_t s) override {
+        return launch(h, k_cg_start<T>, CG_BLOCKS, CG_THREADS, 0, s, 3 * (int64_t)N, static_cast<const T*>(V),
+                      static_cast<const T*>(q), static_cast<T*>(r), static_cast<T*>(p), st, reltol, abstol, maxiter);
+    }
+
+    int cg_iteration(void* x, void* r, void* p, void* q, CgState* st, cudaGraphConditionalHandle loop,
+                     cudaStream_t s) override {
+        const int64_t n = 3 * (int64_t)N;
+        TRY(launch(h, k_cg_direction<T>, CG_BLOCKS, CG_THREADS, 0, s, n, static_cast<const T*>(r),
+                   static_cast<T*>(p), (const CgState*)st));
+        TRY(gather_forces(p, s));
+        TRY(solve(q, s, false, false));
+        TRY(launch(h, k_cg_alpha<T>, CG_BLOCKS, CG_THREADS, 0, s, n, static_cast<const T*>(p),
+                   static_cast<const T*>(q), st));
+        return launch(h, k_cg_update<T>, CG_BLOCKS, CG_THREADS, 0, s, n, static_cast<T*>(x), static_cast<T*>(r),
+                      static_cast<const T*>(p), static_cast<const T*>(q), st, (const int*)h->d_err, loop);
+    }
+
     // keep_u: also leave the velocity grid u = L^-1 S F in gu (the adjoint's
     // only checkpoint); the unfused pipeline leaves it there anyway.
     int solve(void* V, cudaStream_t s, bool keep_u, bool build_lists = true) {
@@ -1198,6 +1258,78 @@ int finish(ffcm_handle* h, cudaStream_t s) {
     return FFCM_OK;
 }
 
+void cg_release(ffcm_handle* h) {
+    auto& c = h->cg;
+    if (c.exec) cudaGraphExecDestroy(c.exec);
+    if (c.graph) cudaGraphDestroy(c.graph);
+    if (c.cs) cudaStreamDestroy(c.cs);
+    for (void* p : {c.x, c.r, c.p, c.q, (void*)c.st})
+        if (p) cudaFree(p);
+    if (c.host) cudaFreeHost(c.host);
+    c = ffcm_handle::Cg{};
+}
+
+// Buffers and the graph of the iteration loop, made once per handle: a gate
+// kernel that sets the loop condition from the start kernel's status, then a
+// while node whose body is one iteration captured on the handle's capture
+// stream. The graph holds only buffers of the handle, so it stays valid
+// across ffcm_set_positions calls (the particle lists are rebuilt outside it).
+int cg_build(ffcm_handle* h) {
+    auto& c = h->cg;
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    for (void** p : {&c.x, &c.r, &c.p, &c.q}) CUDA_TRY(cudaMalloc(p, bytes));
+    CUDA_TRY(cudaMalloc(&c.st, sizeof(CgState)));
+    CUDA_TRY(cudaMemset(c.st, 0, sizeof(CgState)));
+    CUDA_TRY(cudaMallocHost(&c.host, sizeof(CgState)));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c.cs, cudaStreamNonBlocking));
+    CUDA_TRY(cudaGraphCreate(&c.graph, 0));
+    CUDA_TRY(cudaGraphConditionalHandleCreate(&c.loop, c.graph, 0, cudaGraphCondAssignDefault));
+    cudaGraphNode_t gate = nullptr, loop = nullptr;
+    {
+        const CgState* st = c.st;
+        cudaGraphConditionalHandle lh = c.loop;
+        void* args[] = {(void*)&st, (void*)&lh};
+        cudaKernelNodeParams kp = {};
+        kp.func = (void*)k_cg_gate;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(32);
+        kp.kernelParams = args;
+        CUDA_TRY(cudaGraphAddKernelNode(&gate, c.graph, nullptr, 0, &kp));
+    }
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = c.loop;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    CUDA_TRY(cudaGraphAddNode(&loop, c.graph, &gate, 1, &np));
+    cudaGraph_t body = np.conditional.phGraph_out[0];
+    // event records are not allowed in a conditional body: no stage timing
+    const bool prof = h->profiling;
+    h->profiling = false;
+    CUDA_TRY(cudaStreamBeginCaptureToGraph(c.cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const int64_t launches0 = h->launches;
+    const int rc = h->eng->cg_iteration(c.x, c.r, c.p, c.q, c.st, c.loop, c.cs);
+    c.body_kernels = h->launches - launches0;
+    const std::string msg = g_err;
+    const cudaError_t ce = cudaStreamEndCapture(c.cs, &body);
+    h->profiling = prof;
+    if (rc != FFCM_OK) return fail(rc, "capture of the conjugate-gradient iteration failed: " + msg);
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture (conjugate-gradient iteration)");
+    CUDA_TRY(cudaGraphInstantiate(&c.exec, c.graph, 0));
+    return FFCM_OK;
+}
+
+int cg_prepare(ffcm_handle* h) {
+    if (h->cg.exec) return FFCM_OK;
+    const int rc = cg_build(h);
+    if (rc != FFCM_OK) {
+        const std::string msg = g_err;
+        cg_release(h);
+        return fail(rc, msg);
+    }
+    return FFCM_OK;
+}
+
 template <typename T>
 int create_T(ffcm_handle* h, const double* L, double R_c, double a, double ratio, double mu) {
     auto e = std::make_unique<Engine<T>>();
@@ -1310,6 +1442,7 @@ int ffcm_destroy(ffcm_handle* h) {
     if (!h) return FFCM_OK;
     DeviceGuard g(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    cg_release(h);
     h->eng.reset();
     for (cudaEvent_t e : h->events) cudaEventDestroy(e);
     if (h->d_err) cudaFree(h->d_err);
@@ -1641,6 +1774,68 @@ int ffcm_mobility_apply(ffcm_handle* h, void* V, const void* F, int32_t memory, 
         }
         return finish(h, s);
     }
+    return FFCM_OK;
+}
+
+int ffcm_cg_solve(ffcm_handle* h, void* F, const void* V, int32_t memory, double reltol, double abstol,
+                  int32_t maxiter, int32_t flags, int32_t* iterations, double* residual, int32_t* cg_status,
+                  void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    TRY(check_memory(memory));
+    if (!F || !V) return fail(FFCM_ERR_ARGUMENT, "F and V must not be NULL");
+    if (flags & ~FFCM_CG_INITIAL_GUESS) return fail(FFCM_ERR_ARGUMENT, "unknown flag bits");
+    if (!(abstol >= 0) || std::isnan(reltol) || std::isinf(reltol) || std::isinf(abstol))
+        return fail(FFCM_ERR_ARGUMENT, "abstol must be finite and non-negative, reltol finite");
+    if (!h->positions)
+        return fail(FFCM_ERR_STATE,
+                    "ffcm_cg_solve needs the cell list of a preceding ffcm_set_positions on this handle, "
+                    "with no other solve or step call in between");
+    h->ckpt = false;
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    if (reltol < 0) reltol = h->dtype == FFCM_FLOAT32 ? std::sqrt((double)std::numeric_limits<float>::epsilon())
+                                                      : std::sqrt(std::numeric_limits<double>::epsilon());
+    if (maxiter < 0) maxiter = (int32_t)std::min<int64_t>(3 * h->N, INT32_MAX);
+    TRY(e->ensure_lists(s));
+    TRY(cg_prepare(h));
+    auto& c = h->cg;
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    const cudaMemcpyKind in = memory == FFCM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    const cudaMemcpyKind out = memory == FFCM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+    const void* Vd = V;
+    if (memory == FFCM_HOST) {
+        StageScope sc(h, FFCM_STAGE_H2D, s);
+        CUDA_TRY(cudaMemcpyAsync(e->V_out(), V, bytes, in, s));
+        Vd = e->V_out();
+    }
+    const void* q = nullptr;
+    if (flags & FFCM_CG_INITIAL_GUESS) {
+        {
+            StageScope sc(h, FFCM_STAGE_H2D, s);
+            CUDA_TRY(cudaMemcpyAsync(c.x, F, bytes, in, s));
+        }
+        TRY(e->apply_fixed(c.q, c.x, s));
+        q = c.q;
+    } else {
+        CUDA_TRY(cudaMemsetAsync(c.x, 0, bytes, s));
+    }
+    TRY(e->cg_start(Vd, q, c.r, c.p, c.st, reltol, abstol, maxiter, s));
+    CUDA_TRY(cudaGraphLaunch(c.exec, s));
+    {
+        StageScope sc(h, FFCM_STAGE_D2H, s);
+        CUDA_TRY(cudaMemcpyAsync(F, c.x, bytes, out, s));
+    }
+    CUDA_TRY(cudaMemcpyAsync(c.host, c.st, sizeof(CgState), cudaMemcpyDeviceToHost, s));
+    TRY(finish(h, s));
+    // kernels the graph ran: the gate plus one iteration body per iteration
+    h->launches += 1 + (int64_t)c.host->iter * c.body_kernels;
+    if (iterations) *iterations = c.host->iter;
+    if (residual) *residual = std::sqrt(c.host->rr);
+    if (cg_status) *cg_status = c.host->status;
+    if (c.host->status == CG_DEVICE_ERROR)
+        return fail(FFCM_ERR_CUDA, "a kernel of the mobility application raised its device error flag");
     return FFCM_OK;
 }
 

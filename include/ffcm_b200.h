@@ -182,6 +182,31 @@ int ffcm_set_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stre
  * on the handle since. */
 int ffcm_mobility_apply(ffcm_handle* h, void* V, const void* F, int32_t memory, void* stream);
 
+/* ---- resistance problem (conjugate gradients on the operator) -------------
+ * Solves M(Y) F = V for F, M the operator of the last ffcm_set_positions,
+ * by conjugate gradients run on the device: the whole iteration loop is one
+ * CUDA-graph launch (a while node whose condition the device sets), with no
+ * host round trip per iteration. Replaces `cg(M, V)` / `cg!(F, M, V)` of a
+ * Julia Krylov package on FFCMMobility, which the reference declares
+ * symmetric positive definite for this use (src/mobility.jl:161-162).
+ * Iteration and stopping rule as IterativeSolvers.jl's cg: stop once
+ * |r| <= max(reltol |r0|, abstol) or after maxiter iterations, r0 = V - M F0.
+ *   F        3xN: the initial guess F0 when flags has FFCM_CG_INITIAL_GUESS
+ *            (else F0 = 0, initially_zero = true); the solution on return
+ *   reltol   < 0 selects sqrt(eps(T)), IterativeSolvers' default
+ *   maxiter  < 0 selects 3N (size(M, 2)), IterativeSolvers' default
+ *   iterations, residual (|r| of the recursion), cg_status (FFCM_CG_*): any
+ *            may be NULL.
+ * Synchronous on `stream`. FFCM_ERR_STATE without a preceding
+ * ffcm_set_positions; the positions stay set for further applies/solves. */
+#define FFCM_CG_INITIAL_GUESS 1
+#define FFCM_CG_CONVERGED 1
+#define FFCM_CG_MAXITER 2
+#define FFCM_CG_BREAKDOWN 3 /* p.q <= 0 or non-finite: the operator is not SPD on these inputs */
+int ffcm_cg_solve(ffcm_handle* h, void* F, const void* V, int32_t memory, double reltol, double abstol,
+                  int32_t maxiter, int32_t flags, int32_t* iterations, double* residual, int32_t* cg_status,
+                  void* stream);
+
 /* ---- buffer access (step isolation, as test/cuda/ does) ------------------ */
 int64_t ffcm_buffer_bytes(const ffcm_handle* h, int32_t which);
 int ffcm_get_buffer(ffcm_handle* h, int32_t which, void* dst, int64_t nbytes, int32_t memory,

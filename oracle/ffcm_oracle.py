@@ -458,6 +458,64 @@ def objective_gradient(cfg, Y, F, V_target):
 
 
 # ----------------------------------------------------------------------------
+# Resistance problem M(Y) F = V by conjugate gradients. The reference ships no
+# solver; it declares FFCMMobility symmetric positive definite
+# (src/mobility.jl:161-162) so that Julia Krylov packages accept it. This
+# restates the unpreconditioned Hestenes-Stiefel iteration in the order and
+# with the stopping rule of IterativeSolvers.jl 0.9's `cg` (third-party):
+# stop once |r| <= max(reltol |r0|, abstol) or after maxiter iterations.
+# Scalars are double; vectors are kept in T, each update rounded once.
+# ----------------------------------------------------------------------------
+
+def cg(cfg, Y, V, *, reltol=None, abstol=0.0, maxiter=None, x0=None):
+    """-> (F, iters, |r| of the recursion, status) with status 'converged',
+    'maxiter' or 'breakdown'."""
+    T = cfg.T
+    f64 = np.float64
+    if reltol is None:
+        reltol = math.sqrt(float(np.finfo(T).eps))
+    if maxiter is None:
+        maxiter = 3 * cfg.N
+    b = np.asarray(V, T)
+    if x0 is None:
+        x = np.zeros((cfg.N, 3), T)
+        r = b.copy()
+    else:
+        x = np.asarray(x0, T).copy()
+        r = (b - apply(cfg, Y, x)).astype(T)
+    p = np.zeros_like(x)
+    rr = float(np.sum(r.astype(f64) ** 2))
+    thresh = max(reltol * math.sqrt(rr), abstol)
+    if not math.isfinite(rr):
+        return x, 0, math.sqrt(rr), "breakdown"
+    if math.sqrt(rr) <= thresh:
+        return x, 0, math.sqrt(rr), "converged"
+    if maxiter <= 0:
+        return x, 0, math.sqrt(rr), "maxiter"
+    beta = 0.0
+    it = 0
+    while True:
+        p = (r.astype(f64) + beta * p.astype(f64)).astype(T)
+        q = apply(cfg, Y, p)
+        pq = float(np.sum(p.astype(f64) * q.astype(f64)))
+        if not (pq > 0 and math.isfinite(pq)):
+            return x, it, math.sqrt(rr), "breakdown"
+        alpha = rr / pq
+        x = (x.astype(f64) + alpha * p.astype(f64)).astype(T)
+        r = (r.astype(f64) - alpha * q.astype(f64)).astype(T)
+        rr_new = float(np.sum(r.astype(f64) ** 2))
+        beta = rr_new / rr
+        rr = rr_new
+        it += 1
+        if not math.isfinite(rr):
+            return x, it, math.sqrt(rr), "breakdown"
+        if math.sqrt(rr) <= thresh:
+            return x, it, math.sqrt(rr), "converged"
+        if it >= maxiter:
+            return x, it, math.sqrt(rr), "maxiter"
+
+
+# ----------------------------------------------------------------------------
 # Closed-form references used by the reference's own tests
 # ----------------------------------------------------------------------------
 

@@ -1,0 +1,151 @@
+"""The device-side conjugate-gradient resistance solve (`ffcm_cg_solve`, one
+CUDA-graph launch per solve) against the oracle's restatement of the same
+iteration (`ffcm_oracle.cg`, itself pinned against a dense solve on the CPU).
+
+Float64 solves follow the oracle iteration for iteration: the same count and
+the same solution to far below the stopping tolerance. Float32 solves reach
+their default tolerance sqrt(eps) and agree with the Float64 solution to the
+accuracy Float32 grids allow. The host and device memory paths and repeated
+solves agree to the accuracy of the precision, and the operator stays usable
+for `M * F` after a solve.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import ffcm_oracle as O
+from fixtures import nonoverlapping_uniform
+from gpu_helpers import both, kw_of, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(ffcm, T, N, L, M, seed, M_G=8, R_c=3.0):
+    prod, ora = both(ffcm, T, **kw_of(L, N, M, M_G=M_G, R_c=R_c))
+    Y = nonoverlapping_uniform(N, (L, L, L), seed=seed).astype(T)
+    V = np.random.default_rng(seed + 1).standard_normal((N, 3)).astype(T)
+    return prod, ora, Y, V
+
+
+# (N, L, M, M_G): the slab pipeline at 32^3 and 64^3 (the reference's CPU case
+# L = 40, N = 2000), and the generic pipeline (M_G = 6)
+CASES = [(400, 24.0, 32, 8), (2000, 40.0, 64, 8), (300, 24.0, 32, 6)]
+
+
+@pytest.mark.parametrize("N,L,M,MG", CASES)
+def test_cg_f64_follows_the_oracle_iteration(ffcm, N, L, M, MG):
+    prod, ora, Y, V = _system(ffcm, np.float64, N, L, M, seed=N + M, M_G=MG)
+    op = ffcm.FFCMMobility(prod, Y)
+    F, hist = ffcm.cg(op, V, reltol=1e-10, log=True)
+    Fo, it_o, res_o, st_o = O.cg(ora, Y, V, reltol=1e-10)
+    assert hist.isconverged and st_o == "converged"
+    assert abs(hist.iters - it_o) <= 1
+    assert rel_l2(F, Fo) < 1e-8
+    assert hist.resnorm <= 1e-10 * np.linalg.norm(V)
+    # the true residual through the oracle's own operator
+    assert rel_l2(O.apply(ora, Y, F), V) < 1e-9
+
+
+@pytest.mark.parametrize("N,L,M,MG", CASES[:2])
+def test_cg_f32_reaches_its_default_tolerance(ffcm, N, L, M, MG):
+    prod, _, Y, V = _system(ffcm, np.float32, N, L, M, seed=2 * N + M, M_G=MG)
+    ora64 = O.OracleConfig(np.float64, **kw_of(L, N, M, M_G=MG, R_c=3.0))
+    F, hist = ffcm.cg(ffcm.FFCMMobility(prod, Y), V, log=True)
+    assert hist.isconverged
+    assert hist.resnorm <= math.sqrt(np.finfo(np.float32).eps) * np.linalg.norm(V.astype(np.float64))
+    F64, _, _, st = O.cg(ora64, Y.astype(np.float64), V.astype(np.float64), reltol=1e-10)
+    assert st == "converged"
+    assert rel_l2(F, F64) < 2e-3
+    assert rel_l2(O.apply(ora64, Y.astype(np.float64), F.astype(np.float64)), V) < 2e-3
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+def test_cg_single_iteration_is_the_steepest_descent_step(ffcm, T):
+    N, L, M = 400, 24.0, 32
+    prod, ora, Y, V = _system(ffcm, T, N, L, M, seed=21)
+    F, hist = ffcm.cg(ffcm.FFCMMobility(prod, Y), V, reltol=0.0, maxiter=1, log=True)
+    assert (hist.iters, hist.status) == (1, "maxiter")
+    Fo, it, res, st = O.cg(ora, Y, V, reltol=0.0, maxiter=1)
+    assert (it, st) == (1, "maxiter")
+    assert rel_l2(F, Fo) < (2e-6 if T == np.float32 else 1e-12)
+    assert math.isclose(hist.resnorm, res, rel_tol=1e-4 if T == np.float32 else 1e-10)
+
+
+def test_cg_zero_rhs_initial_guess_and_maxiter_zero(ffcm):
+    N, L, M = 400, 24.0, 32
+    prod, ora, Y, V = _system(ffcm, np.float64, N, L, M, seed=31)
+    op = ffcm.FFCMMobility(prod, Y)
+    F, hist = ffcm.cg(op, np.zeros_like(V), log=True)
+    assert (hist.iters, hist.resnorm, hist.status) == (0, 0.0, "converged") and not F.any()
+    Fs, h1 = ffcm.cg(op, V, reltol=1e-12, log=True)
+    # the solution as the initial guess: the first residual already meets abstol
+    F2, h2 = ffcm.cg(op, V, x0=Fs, abstol=1e-8 * np.linalg.norm(V), log=True)
+    assert (h2.iters, h2.status) == (0, "converged")
+    assert np.array_equal(F2, Fs)
+    # warm start from a perturbed solution: relative to |r0|, as IterativeSolvers
+    x0 = Fs + 1e-3 * np.random.default_rng(5).standard_normal(Fs.shape)
+    F3, h3 = ffcm.cg(op, V, x0=x0, reltol=1e-6, log=True)
+    Fo, it_o, _, st_o = O.cg(ora, Y, V, x0=x0, reltol=1e-6)
+    assert h3.isconverged and st_o == "converged" and abs(h3.iters - it_o) <= 1
+    assert rel_l2(F3, Fo) < 1e-8
+    F4, h4 = ffcm.cg(op, V, reltol=1e-12, maxiter=0, log=True)
+    assert (h4.iters, h4.status) == (0, "maxiter") and not F4.any()
+
+
+@pytest.mark.parametrize("T", [np.float32, np.float64])
+def test_cg_repeats_and_memory_paths_agree(ffcm, T):
+    # The interpolation adds each slab's share of a particle's velocity with
+    # atomics, so one operator application is reproducible to rounding, not
+    # bit for bit; the solves agree to the accuracy of T.
+    torch = pytest.importorskip("torch")
+    N, L, M = 2000, 40.0, 64
+    prod, _, Y, V = _system(ffcm, T, N, L, M, seed=41)
+    op = ffcm.FFCMMobility(prod, Y)
+
+    def agree(Fa, ha, Fb, hb):
+        # same iteration count: rounding-level agreement; one more iteration
+        # on one side: agreement to the stopping tolerance sqrt(eps)
+        if ha.iters == hb.iters:
+            return rel_l2(Fa, Fb) < (1e-4 if T == np.float32 else 1e-11)
+        return abs(ha.iters - hb.iters) == 1 and rel_l2(Fa, Fb) < (2e-3 if T == np.float32 else 1e-7)
+
+    F1, h1 = ffcm.cg(op, V, log=True)
+    F2, h2 = ffcm.cg(op, V, log=True)
+    assert agree(F2, h2, F1, h1)
+    Vd = torch.from_numpy(V).cuda()
+    Fd, hd = ffcm.cg(op, Vd, log=True)
+    torch.cuda.synchronize()
+    assert agree(Fd.cpu().numpy(), hd, F1, h1)
+    # device-resident positions give the same operator
+    op_d = ffcm.FFCMMobility(prod, torch.from_numpy(Y).cuda())
+    Fe, he = ffcm.cg(op_d, Vd, log=True)
+    torch.cuda.synchronize()
+    assert agree(Fe.cpu().numpy(), he, F1, h1)
+
+
+def test_operator_after_cg_and_cg_after_another_solve(ffcm):
+    N, L, M = 400, 24.0, 32
+    prod, ora, Y, V = _system(ffcm, np.float64, N, L, M, seed=51)
+    op = ffcm.FFCMMobility(prod, Y)
+    F = ffcm.cg(op, V, reltol=1e-12)
+    assert rel_l2(op @ F, V) < 1e-10                    # M * F on the same operator
+    # a plain solve on the config invalidates the fixed positions; cg re-fixes them
+    other = nonoverlapping_uniform(N, (L, L, L), seed=52)
+    W = np.empty_like(V)
+    ffcm.mobility(W, prod, other, V)
+    F_again = ffcm.cg(op, V, reltol=1e-12)
+    assert rel_l2(F_again, F) < 1e-10
+    # new positions on the same config: the graph is reused, the lists rebuilt
+    op2 = ffcm.FFCMMobility(prod, other)
+    G, hg = ffcm.cg(op2, V, reltol=1e-10, log=True)
+    Go, it_o, _, _ = O.cg(ora, other, V, reltol=1e-10)
+    assert abs(hg.iters - it_o) <= 1 and rel_l2(G, Go) < 1e-8
+
+
+def test_cg_reports_maxiter_when_the_tolerance_is_out_of_reach(ffcm):
+    N, L, M = 400, 24.0, 32
+    prod, ora, Y, V = _system(ffcm, np.float32, N, L, M, seed=61)
+    F, hist = ffcm.cg(ffcm.FFCMMobility(prod, Y), V, reltol=1e-12, maxiter=40, log=True)
+    assert hist.status == "maxiter" and hist.iters == 40 and not hist.isconverged
+    assert np.all(np.isfinite(F))
