@@ -103,6 +103,76 @@ __device__ __forceinline__ void fft_line_regs(cplx<T> (&v)[8], int j, const Exch
     }
 }
 
+// v *= (cr + i ci), or by its conjugate when inv
+template <typename T>
+__device__ __forceinline__ cplx<T> cmul_const(cplx<T> v, T cr, T ci, bool inv) {
+    if (inv) ci = -ci;
+    return cplx<T>{v.x * cr - v.y * ci, v.x * ci + v.y * cr};
+}
+
+// 16-point DFT in registers, 16 = 4 x 4: with q = b + 4a and k = c + 4d,
+// X[c + 4d] = sum_b W4^(bd) [W16^(bc) sum_a v[b + 4a] W4^(ac)].
+template <typename T>
+__device__ __forceinline__ void dft16(cplx<T> (&v)[16], bool inv) {
+#pragma unroll
+    for (int b = 0; b < 4; ++b) dft4(v[b], v[b + 4], v[b + 8], v[b + 12], inv);   // v[b + 4c] = Y_b[c]
+    // W16^e = exp(-2 pi i e / 16) for e = bc (forward)
+    const T c8 = T(0.92387953251128675612818318939678828682);   // cos(pi/8)
+    const T s8 = T(0.38268343236508977172845998403039886676);   // sin(pi/8)
+    const T c4 = T(0.70710678118654752440084436210484903928);   // cos(pi/4)
+    v[1 + 4 * 1] = cmul_const(v[1 + 4 * 1], c8, -s8, inv);     // e = 1
+    v[1 + 4 * 2] = cmul_const(v[1 + 4 * 2], c4, -c4, inv);     // e = 2
+    v[1 + 4 * 3] = cmul_const(v[1 + 4 * 3], s8, -c8, inv);     // e = 3
+    v[2 + 4 * 1] = cmul_const(v[2 + 4 * 1], c4, -c4, inv);     // e = 2
+    v[2 + 4 * 2] = inv ? mul_pi(v[2 + 4 * 2]) : mul_mi(v[2 + 4 * 2]);   // e = 4
+    v[2 + 4 * 3] = cmul_const(v[2 + 4 * 3], -c4, -c4, inv);    // e = 6
+    v[3 + 4 * 1] = cmul_const(v[3 + 4 * 1], s8, -c8, inv);     // e = 3
+    v[3 + 4 * 2] = cmul_const(v[3 + 4 * 2], -c4, -c4, inv);    // e = 6
+    v[3 + 4 * 3] = cmul_const(v[3 + 4 * 3], -c8, s8, inv);     // e = 9
+    cplx<T> out[16];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        cplx<T> a0 = v[4 * c], a1 = v[4 * c + 1], a2 = v[4 * c + 2], a3 = v[4 * c + 3];
+        dft4(a0, a1, a2, a3, inv);
+        out[c] = a0;
+        out[c + 4] = a1;
+        out[c + 8] = a2;
+        out[c + 12] = a3;
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) v[k] = out[k];
+}
+
+// 256-point FFT of a line held by 16 consecutive lanes (two lines per warp;
+// the x transforms of the slab kernels at x length 512). 256 = 16 x 16,
+// decimation in time: thread t (0..15) holds z[t + 16 q] on entry; a 16-point
+// DFT over q in registers, the twiddle W256^(t k1), one exchange through the
+// line's scratch `xb` (16 x 17 complex; may alias the line's own input, which
+// is read before), and a 16-point DFT over t. On exit thread t holds
+// Z[t + 16 k2], the same positions as on entry. `tw` holds W_n^e at e * tws
+// (tws = 2 for a table of 512). Lanes of both lines of the warp must call it
+// together.
+template <typename T>
+__device__ __forceinline__ void fft256_h16(cplx<T> (&v)[16], int t, cplx<T>* xb, const cplx<T>* tw, int tws,
+                                           bool inv) {
+    dft16(v, inv);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], twid(tw, t * k1, tws, inv));
+    __syncwarp();
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) xb[k1 * 17 + t] = v[k1];
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 16; ++j) v[j] = xb[t * 17 + j];
+    dft16(v, inv);
+}
+
+// Value of lane `src` (0..15) of this lane's 16-lane half of the warp.
+template <typename T>
+__device__ __forceinline__ cplx<T> shfl16(cplx<T> v, int src) {
+    return cplx<T>{__shfl_sync(0xffffffffu, v.x, src, 16), __shfl_sync(0xffffffffu, v.y, src, 16)};
+}
+
 // Copy a twiddle table into shared memory.
 template <typename T>
 __device__ __forceinline__ void load_table(cplx<T>* dst, const cplx<T>* __restrict__ src, int count) {

@@ -273,7 +273,7 @@ __device__ __forceinline__ void spread_put(const StencilParams<T>& p, SpreadWin<
 
 // ---- spread into a slab, then x-r2c straight into the spectrum -----------
 template <typename T, int H, int BY, int BZ>
-__global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__ Ys,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(const vec4<T>* __restrict__ Ys,
                                                      const vec4<T>* __restrict__ Fs,
                                                      const int32_t* __restrict__ off,
                                                      cplx<T>* __restrict__ spec, int hxp,
@@ -419,6 +419,34 @@ __global__ void __launch_bounds__(256) k_spread_slab(const vec4<T>* __restrict__
         if (count > 0) process(count);
         __syncthreads();
     }
+    if constexpr (H == 256 && sizeof(T) == 4) {
+        // x length 512: 16 threads per row, two rows per warp (ROWS is even,
+        // so a warp's two rows are both present or both absent); the row is
+        // its own exchange scratch; the r2c split takes Z[H - k] from the
+        // partner lane by shuffle
+        const int t = threadIdx.x & 15;
+        for (int r = (int)(threadIdx.x >> 4); r < ROWS; r += (int)(blockDim.x >> 4)) {
+            cplx<T>* rowc = reinterpret_cast<cplx<T>*>(acc + r * P);
+            cplx<T> v[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) v[q] = rowc[t + 16 * q];
+            fft256_h16(v, t, rowc, tw, 2, false);
+            const int c = r / NRP, bd = r % NRP;
+            const int b = bd % BY, d = bd / BY;
+            cplx<T>* dst = spec + (((int64_t)c * p.Mz + z0r + d) * p.My + y0r + b) * hxp;
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int k = t + 16 * q;
+                const cplx<T> other = shfl16(v[15 - q], (16 - t) & 15);
+                const cplx<T> Zk = v[q];
+                const cplx<T> Zc = cconj(t == 0 ? v[(16 - q) & 15] : other);
+                const cplx<T> S = cadd(Zk, Zc), D = cmul(tw[k], csub(Zk, Zc));
+                dst[k] = cplx<T>{T(0.5) * (S.x + D.y), T(0.5) * (S.y - D.x)};
+            }
+            if (t == 0) dst[H] = cplx<T>{v[0].x - v[0].y, T(0)};
+        }
+        return;
+    }
     // x r2c of every slab row (H/8 threads per row), output straight to spec.
     // A row that fits one warp is transformed with warp-level synchronisation
     // only (rows are disjoint between warps; idle lanes exchange through a
@@ -474,7 +502,7 @@ __host__ __device__ constexpr unsigned slab_row_copy_bytes() {
 }
 
 template <typename T, int H, int BY, int BZ>
-__global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__ Ys,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(const vec4<T>* __restrict__ Ys,
                                                      const int32_t* __restrict__ off,
                                                      const cplx<T>* __restrict__ spec, int hxp,
                                                      T* __restrict__ Vs, StencilParams<T> p,
@@ -513,6 +541,31 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
         mbar_wait_bounded(&bar, 0, 1 << 22);
         return;
     }
+    if constexpr (H == 256 && sizeof(T) == 4) {
+        // x length 512: 16 threads per row, two rows per warp (see the spread)
+        const int t = threadIdx.x & 15;
+        for (int r = (int)(threadIdx.x >> 4); r < ROWS; r += (int)(blockDim.x >> 4)) {
+            cplx<T>* rowc = reinterpret_cast<cplx<T>*>(acc + r * P);
+            cplx<T> v[16];
+#pragma unroll
+            for (int q = 0; q < 16; ++q) {
+                const int k = t + 16 * q;
+                cplx<T> Xk = rowc[k];
+                cplx<T> Xc = rowc[H - k];
+                if (k == 0) {
+                    Xk.y = T(0);
+                    Xc.y = T(0);
+                }
+                const cplx<T> A = cadd(Xk, cconj(Xc));
+                const cplx<T> B = cmul(csub(Xk, cconj(Xc)), cconj(tw[k]));
+                v[q] = cadd(A, mul_pi(B));
+            }
+            fft256_h16(v, t, rowc, tw, 2, true);
+            __syncwarp();   // the exchange reads of both rows are done
+#pragma unroll
+            for (int q = 0; q < 16; ++q) rowc[t + 16 * q] = v[q];   // real row, unpadded
+        }
+    } else {
     constexpr int TPL = H / 8, Q = H / 8;
     constexpr bool WARP = TPL <= 32;
     const int lines_per_round = blockDim.x / TPL;
@@ -544,6 +597,7 @@ __global__ void __launch_bounds__(256) k_interp_slab(const vec4<T>* __restrict__
             for (int qq = 0; qq < 8; ++qq) rowc[j + qq * Q] = v[qq];   // real row, unpadded
         }
         if (WARP) __syncwarp(); else __syncthreads();
+    }
     }
     __syncthreads();
     // one thread per particle: weights in registers, gather over the slab rows
