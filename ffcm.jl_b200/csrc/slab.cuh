@@ -11,11 +11,12 @@
 //  * k_spread_slab: the list is replayed in windows of SLAB_CAP entries; one
 //    thread per entry stores the entry's per-row weights gy gz and r^2 parts
 //    (src/stencil.jl:80-112); the window is ordered by the first x point of
-//    each stencil, and each thread then owns grid points x and gathers
-//    F (a0 + a2 r^2) gx gy gz from the entries covering x into registers
-//    (src/spread_forces.jl:73-130; gx is evaluated by the one thread that
-//    uses it) — no atomics, deterministic. Each slab row is then x-r2c
-//    transformed in shared memory and written straight to the spectrum.
+//    each stencil (a stable counting sort), and each thread then owns grid
+//    points x and gathers F (a0 + a2 r^2) gx gy gz from the entries covering
+//    x into registers (src/spread_forces.jl:73-130; gx is evaluated by the
+//    one thread that uses it) — no floating-point atomics, deterministic.
+//    Each slab row is then x-r2c transformed in shared memory and written
+//    straight to the spectrum.
 //  * k_interp_slab: the slab's spectrum rows are x-c2r transformed into shared
 //    memory; one thread per listed particle gathers its partial velocity over
 //    the slab rows from registers (src/interpolate.jl:322-376) and adds it,
@@ -237,8 +238,8 @@ struct SpreadWin {
     // rows padded by one element: lanes reading different entries at the same
     // slab row then fall into different banks
     T gyz[SLAB_CAP][NRP + 1], dyz[SLAB_CAP][NRP + 1];   // gy gz and gy gz (r2y + r2z)
-    unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry)
-    int first[2 * H + 1];     // first sorted entry with key >= v
+    unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry), in sorted order
+    int first[2 * H + 1];     // counting-sort bins: entries with key <= v
     int scan[32];
 };
 
@@ -292,31 +293,54 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
     load_table(tw, twx, Mx);
     const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
-    for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
-    __syncthreads();
+    // the first window stores its sums (every grid point of every row is
+    // owned by one thread), later windows add; a slab without particles is
+    // zeroed after the window loop
+    bool fresh = true;
     // Window entries [0, count) are in W; all threads call this after a barrier.
     auto process = [&](int count) {
-        // order the window by first x point: each entry's rank is the number
-        // of entries with a smaller (key, index) pair
-        for (int i = threadIdx.x; i < SLAB_CAP; i += blockDim.x) {
-            if (i < count) {
-                const unsigned me = ((unsigned)W.key[i] << 7) | (unsigned)i;
-                int rank = 0;
-                for (int k = 0; k < count; ++k) rank += (((unsigned)W.key[k] << 7) | (unsigned)k) < me;
-                W.sk[rank] = me;
-            } else {
-                W.sk[i] = 0xffffffffu;
+        // order the window by first x point, stably in entry order: a
+        // counting sort (per-key counts, exclusive scan, then one warp places
+        // the entries in index order, advancing a per-key cursor). After it
+        // fe[v] = number of entries with key <= v, the end of key v's run.
+        int* fe = W.first;
+        for (int v = threadIdx.x; v < Mx; v += blockDim.x) fe[v] = 0;
+        __syncthreads();
+        if ((int)threadIdx.x < count) atomicAdd(&fe[W.key[threadIdx.x]], 1);
+        __syncthreads();
+        {
+            constexpr int BPT = (Mx + 255) / 256;   // bins per thread (256 threads)
+            int cnt[BPT], sum = 0;
+#pragma unroll
+            for (int u = 0; u < BPT; ++u) {
+                const int b = (int)threadIdx.x * BPT + u;
+                cnt[u] = b < Mx ? fe[b] : 0;
+                sum += cnt[u];
+            }
+            int tot;
+            int pre = block_scan(sum, W.scan, tot);
+#pragma unroll
+            for (int u = 0; u < BPT; ++u) {
+                const int b = (int)threadIdx.x * BPT + u;
+                if (b < Mx) fe[b] = pre;
+                pre += cnt[u];
             }
         }
         __syncthreads();
-        for (int v = threadIdx.x; v <= Mx; v += blockDim.x) {
-            int lo = 0, hi = SLAB_CAP;   // first sorted entry with key >= v
-            while (lo < hi) {
-                const int mid = (lo + hi) >> 1;
-                if ((int)(W.sk[mid] >> 7) < v) lo = mid + 1;
-                else hi = mid;
+        if (threadIdx.x < 32) {
+            const unsigned lane = threadIdx.x;
+            for (int c0 = 0; c0 < count; c0 += 32) {
+                const int i = c0 + (int)lane;
+                const bool act = i < count;
+                const int key = act ? W.key[i] : -1 - (int)lane;   // inactive lanes: unique keys
+                const unsigned grp = __match_any_sync(0xffffffffu, key);
+                const int below = __popc(grp & ((1u << lane) - 1u));
+                const int pos = act ? fe[key] + below : 0;
+                __syncwarp();
+                if (act && below == __popc(grp) - 1) fe[key] += __popc(grp);
+                if (act) W.sk[pos] = ((unsigned)key << 7) | (unsigned)i;
+                __syncwarp();
             }
-            W.first[v] = lo;
         }
         __syncthreads();
         // gather: each thread owns grid points x of all slab rows
@@ -331,12 +355,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
             for (int part = 0; part < 2; ++part) {
                 int kb, ke;
                 if (part == 0) {
-                    kb = W.first[lo1 >= 0 ? lo1 : 0];
-                    ke = W.first[x + 1];
+                    kb = lo1 > 0 ? fe[lo1 - 1] : 0;
+                    ke = fe[x];
                 } else {
                     if (lo1 >= 0) break;
-                    kb = W.first[Mx + lo1];
-                    ke = W.first[Mx];
+                    kb = fe[Mx + lo1 - 1];
+                    ke = fe[Mx - 1];
                 }
                 for (int kk = kb; kk < ke; ++kk) {
                     const unsigned v = W.sk[kk];
@@ -364,11 +388,19 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
                         }
                 }
             }
+            if (fresh) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c)
+                for (int c = 0; c < 3; ++c)
 #pragma unroll
-                for (int r = 0; r < NRP; ++r) acc[(c * NRP + r) * P + x] += a[c][r];
+                    for (int r = 0; r < NRP; ++r) acc[(c * NRP + r) * P + x] = a[c][r];
+            } else {
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int r = 0; r < NRP; ++r) acc[(c * NRP + r) * P + x] += a[c][r];
+            }
         }
+        fresh = false;
     };
     const int stored = counts[cta];
     if (stored >= 0) {
@@ -417,6 +449,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
             }
         }
         if (count > 0) process(count);
+        __syncthreads();
+    }
+    if (fresh) {   // no particle reaches the slab (block-uniform)
+        for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
         __syncthreads();
     }
     if constexpr (H == 256 && sizeof(T) == 4) {

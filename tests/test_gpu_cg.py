@@ -104,10 +104,11 @@ def test_cg_repeats_and_memory_paths_agree(ffcm, T):
     op = ffcm.FFCMMobility(prod, Y)
 
     def agree(Fa, ha, Fb, hb):
-        # same iteration count: rounding-level agreement; one more iteration
+        # same iteration count: agreement to rounding amplified by the
+        # iteration (F64: ~1e-16 x condition x iterations); one more iteration
         # on one side: agreement to the stopping tolerance sqrt(eps)
         if ha.iters == hb.iters:
-            return rel_l2(Fa, Fb) < (1e-4 if T == np.float32 else 1e-11)
+            return rel_l2(Fa, Fb) < (1e-4 if T == np.float32 else 1e-9)
         return abs(ha.iters - hb.iters) == 1 and rel_l2(Fa, Fb) < (2e-3 if T == np.float32 else 1e-7)
 
     F1, h1 = ffcm.cg(op, V, log=True)
