@@ -1,5 +1,6 @@
 // Bulk asynchronous copies from global to shared memory (the TMA's untiled
-// form, cp.async.bulk) with an mbarrier for completion. Each block fills only
+// form, cp.async.bulk) with an mbarrier for completion, and the bulk-group
+// bookkeeping of stores from shared to global memory. Each block fills only
 // its own shared memory from this GPU's memory. Addresses and sizes must be
 // multiples of 16 bytes.
 #pragma once
@@ -59,5 +60,18 @@ __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src_global
         "l"(src_global), "r"(bytes), "r"(smem_addr(bar))
         : "memory");
 }
+
+// Bulk stores (shared -> global, the async proxy reading this block's shared
+// memory) are tracked as bulk groups of the issuing thread.
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+
+// The issuing thread waits until its committed bulk stores have finished
+// reading shared memory (the source may then be overwritten).
+__device__ __forceinline__ void bulk_wait_read_all() {
+    asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+}
+
+// The issuing thread waits until its committed bulk stores are complete.
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 
 }  // namespace ffcm

@@ -9,9 +9,15 @@
 // z axes merge because a component's stride is Mz times the z stride -- into
 // a staging buffer, completing on an mbarrier; as soon as the block has moved
 // the tile into registers, the next tile's copy is issued, so it lands while
-// the block transforms. Each block fills only its own shared memory, from this
-// GPU's memory. The x coordinate of every copy is a multiple of B complex
-// values (B even), so it starts on a 16-byte boundary.
+// the block transforms. The transformed tile goes back the same way: the
+// block writes it into its (then idle) exchange region in the staging layout
+// and one thread issues tiled bulk stores through the same tensor map, waited
+// for (reads of shared memory done) before the region is written again. A
+// tile may extend into the padding columns of the spectrum pitch; those are
+// transformed and stored like the others and never read as data. Each block
+// fills and drains only its own shared memory, from and to this GPU's memory.
+// The x coordinate of every copy is a multiple of B complex values (B even),
+// so it starts on a 16-byte boundary.
 #pragma once
 
 #include <cuda.h>
@@ -40,6 +46,17 @@ __device__ __forceinline__ void tma_load_3d(void* dst_smem, const CUtensorMap* m
         : "memory");
 }
 
+// Tiled bulk store of a box from this block's shared memory (128-byte aligned)
+// to the tensor at (x, y, z), as a bulk group of the calling thread. The
+// block's writes of the box must be made visible to the async proxy first
+// (fence_proxy_async_smem by the writers, then a barrier).
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, int x, int y, int z, const void* src_smem) {
+    asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(z), "r"(smem_addr(src_smem))
+                 : "memory");
+}
+
 // block = B * n/8 threads; smem: up to 128 bytes of alignment slack | staging
 // (3 n B, 128-byte aligned) | table (n) | exchange (3 B padded_len(n)).
 template <typename T, int n, int B>
@@ -59,8 +76,6 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
     const int b = threadIdx.x % B, j = threadIdx.x / B;
     const int tiles_x = (kx1 - kx0 + B - 1) / B;
     const int ntiles = tiles_x * My;
-    const int64_t zs = (int64_t)My * hxp;
-    const int64_t cs = (int64_t)n * zs;
     auto issue = [&](int t) {   // one thread, after a barrier
         const int tx = t % tiles_x, y = t / tiles_x;
         fence_proxy_async_smem();   // the block's reads of the staging buffer come first
@@ -76,13 +91,20 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
     __syncthreads();
     const Exchange<T> ex[3] = {Exchange<T>{ex_sm, b, B}, Exchange<T>{ex_sm + B * PL, b, B},
                                Exchange<T>{ex_sm + 2 * B * PL, b, B}};
+    // the result tile leaves through the exchange region, laid out like the
+    // staging buffer ([c n + z][B], 128-byte aligned), by tiled bulk stores
+    cplx<T>* out = ex_sm;
+    static_assert(3 * n * B <= 3 * B * PL, "the result tile must fit the exchange region");
     unsigned phase = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
         const bool landed = mbar_wait_bounded(&bar, phase, 1 << 22);
         if (__syncthreads_or(!landed)) {
             // the tile did not arrive: report, give the copies one more
             // bounded chance to finish, and leave
-            if (threadIdx.x == 0) atomicOr(err, DEVERR_COPY_TIMEOUT);
+            if (threadIdx.x == 0) {
+                atomicOr(err, DEVERR_COPY_TIMEOUT);
+                bulk_wait_all();
+            }
             mbar_wait_bounded(&bar, phase, 1 << 22);
             return;
         }
@@ -91,6 +113,9 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
         for (int c = 0; c < 3; ++c)
 #pragma unroll
             for (int q = 0; q < 8; ++q) v[c][q] = stage[(c * n + j + q * Q) * B + b];
+        // the previous tile's stores have read the exchange region before
+        // anyone writes it again
+        if (threadIdx.x == 0) bulk_wait_read_all();
         __syncthreads();   // the staging buffer is free for the next tile
         if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
         const int tx = t % tiles_x, y = t / tiles_x;
@@ -115,17 +140,21 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
             }
         }
         fft_lines_lockstep<T, n, 3>(v, j, ex, tw, true);
-        if (kx < kx1) {
-            cplx<T>* col = spec + (int64_t)y * hxp + kx;
+        __syncthreads();   // every exchange read of the inverse transform is done
 #pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                const int64_t o = (int64_t)(j + q * Q) * zs;
-                col[o] = v[0][q];
-                col[cs + o] = v[1][q];
-                col[2 * cs + o] = v[2][q];
-            }
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) out[(c * n + j + q * Q) * B + b] = v[c][q];
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < NCOPY; ++k)
+                tma_store_3d(&tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, y, k * ZB, out + k * ZB * B);
+            bulk_commit();
         }
     }
+    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 // y pass, same scheme: a tile is B kx columns x all n rows y of one (c, z)
@@ -148,7 +177,6 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_y(const __grid_constant__ 
     const int b = threadIdx.x % B, j = threadIdx.x / B;
     const int tiles_x = (kx1 - kx0 + B - 1) / B;
     const int ntiles = tiles_x * Mz * 3;
-    const int64_t plane_elems = (int64_t)n * hxp;
     auto issue = [&](int t) {   // one thread, after a barrier
         const int tx = t % tiles_x, pz = t / tiles_x;
         fence_proxy_async_smem();   // the block's reads of the staging buffer come first
@@ -163,28 +191,42 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_y(const __grid_constant__ 
     }
     __syncthreads();
     const Exchange<T> ex[1] = {Exchange<T>{ex_sm, b, B}};
+    // the result tile leaves through the exchange region ([y][B], 128-byte
+    // aligned) by tiled bulk stores
+    cplx<T>* out = ex_sm;
+    static_assert(n * B <= B * padded_len(n), "the result tile must fit the exchange region");
     unsigned phase = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
         const bool landed = mbar_wait_bounded(&bar, phase, 1 << 22);
         if (__syncthreads_or(!landed)) {
-            if (threadIdx.x == 0) atomicOr(err, DEVERR_COPY_TIMEOUT);
+            if (threadIdx.x == 0) {
+                atomicOr(err, DEVERR_COPY_TIMEOUT);
+                bulk_wait_all();
+            }
             mbar_wait_bounded(&bar, phase, 1 << 22);
             return;
         }
         cplx<T> v[1][8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) v[0][q] = stage[(j + q * Q) * B + b];
+        if (threadIdx.x == 0) bulk_wait_read_all();   // the previous tile's stores left the exchange region
         __syncthreads();   // the staging buffer is free for the next tile
         if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
         fft_lines_lockstep<T, n, 1>(v, j, ex, tw, inverse != 0);
         const int tx = t % tiles_x, pz = t / tiles_x;
-        const int kx = kx0 + tx * B + b;
-        if (kx < kx1) {
-            cplx<T>* dst = spec + (int64_t)pz * plane_elems + kx;
+        __syncthreads();   // every exchange read of the transform is done
 #pragma unroll
-            for (int q = 0; q < 8; ++q) dst[(int64_t)(j + q * Q) * hxp] = v[0][q];
+        for (int q = 0; q < 8; ++q) out[(j + q * Q) * B + b] = v[0][q];
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < NCOPY; ++k)
+                tma_store_3d(&tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, k * YB, pz, out + k * YB * B);
+            bulk_commit();
         }
     }
+    if (threadIdx.x == 0) bulk_wait_all();
 }
 
 template <typename T>
