@@ -179,15 +179,38 @@ def ncu_traffic(stage):
     return None
 
 
-def cpu_baseline_run(Y, F, threads):
+def cpu_baseline_run(Y, F, threads, keep=None):
     """One full solve of the workload by the CPU oracle (particle loops serial as
-    in the reference, FFT with `threads` workers as fft_threads)."""
+    in the reference, FFT with `threads` workers as fft_threads). With `keep`
+    (a list), the oracle's velocities are appended to it."""
     import ffcm_oracle as O
     cfg = O.OracleConfig(np.float32, **config_kwargs(), fft_threads=threads)
     V = np.zeros_like(Y)
     t0 = time.perf_counter()
     O.mobility(V, cfg, Y, F)
-    return time.perf_counter() - t0
+    sec = time.perf_counter() - t0
+    if keep is not None:
+        keep.append(V)
+    return sec
+
+
+def accuracy_report(V, Y, F, V32, threads):
+    """Errors of the GPU velocities against the oracle: rel-L2 and max-abs
+    against the Float64 restatement, rel-L2 against the Float32 one."""
+    import ffcm_oracle as O
+    cfg = O.OracleConfig(np.float64, **config_kwargs(), fft_threads=threads)
+    V64 = O.apply(cfg, Y.astype(np.float64), F.astype(np.float64))
+    V = np.asarray(V, np.float64)
+    d64 = V - V64
+    return {"rel_l2_vs_oracle_f64": float(np.linalg.norm(d64) / np.linalg.norm(V64)),
+            "max_abs_vs_oracle_f64": float(np.abs(d64).max()),
+            "max_abs_oracle_f64": float(np.abs(V64).max()),
+            "rel_l2_vs_oracle_f32": float(np.linalg.norm(V - V32) / np.linalg.norm(V32)),
+            # the Float32 restatement's own distance from Float64: the floor any
+            # Float32 implementation of the reference sits at on this workload
+            "oracle_f32_rel_l2_vs_oracle_f64": float(np.linalg.norm(np.asarray(V32, np.float64) - V64)
+                                                     / np.linalg.norm(V64)),
+            "targets": "rel-L2 <= 1e-4 vs Float64, <= 1e-5 vs the Float32 restatement"}
 
 
 def run_reference(args, rank, world):
@@ -374,14 +397,17 @@ def run_ours(args, rank, world, local_rank):
         traffic = ncu_traffic(dom)
         # CPU baseline: one full solve of the workload by the oracle on the host
         cpu_threads = os.cpu_count() or 1
+        accuracy = None
         if args.skip_cpu_baseline:
             cpu = None
         else:
-            sec = cpu_baseline_run(Y, F, cpu_threads)
+            kept = []
+            sec = cpu_baseline_run(Y, F, cpu_threads, keep=kept)
             cpu = {"value": N / sec, "unit": UNIT, "cores": cpu_threads, "kind": "port",
                    "sample": "one full solve of the workload by the C/pocketfft restatement of "
                              "the reference CPU path; particle loops serial as in the reference, "
                              f"FFT on {cpu_threads} threads (fft_threads)"}
+            accuracy = accuracy_report(Vh.numpy(), Y, F, kept[0], cpu_threads)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -400,6 +426,7 @@ def run_ours(args, rank, world, local_rank):
                                "frac": solve_bytes / (ms / 1e3) / 1e9 / peak},
             "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
             "cpu_baseline": cpu,
+            "accuracy": accuracy,
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }

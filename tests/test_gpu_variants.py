@@ -22,7 +22,9 @@ CASES = {"64^3": dict(L=(40.0,) * 3, N=2000, M=(64, 64, 64)),
          # x length 1024), spacing and density of the 64^3 case
          "64x64x1024": dict(L=(40.0, 40.0, 640.0), N=32000, M=(64, 64, 1024)),
          "64x1024x64": dict(L=(40.0, 640.0, 40.0), N=32000, M=(64, 1024, 64)),
-         "1024x64x64": dict(L=(640.0, 40.0, 40.0), N=32000, M=(1024, 64, 64))}
+         "1024x64x64": dict(L=(640.0, 40.0, 40.0), N=32000, M=(1024, 64, 64)),
+         # lines of 512 along y
+         "64x512x64": dict(L=(40.0, 320.0, 40.0), N=16000, M=(64, 512, 64))}
 Y_VARIANTS = [(k, B) for k in (0, 1, 2) for B in (2, 4, 8, 16)]
 Z_VARIANTS = [(k, B) for k in (0, 1, 2, 3) for B in (2, 4, 8, 16)]
 
