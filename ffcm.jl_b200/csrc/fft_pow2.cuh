@@ -143,34 +143,55 @@ __device__ __forceinline__ void dft16(cplx<T> (&v)[16], bool inv) {
     for (int k = 0; k < 16; ++k) v[k] = out[k];
 }
 
-// 256-point FFT of a line held by 16 consecutive lanes (two lines per warp;
-// the x transforms of the slab kernels at x length 512). 256 = 16 x 16,
-// decimation in time: thread t (0..15) holds z[t + 16 q] on entry; a 16-point
-// DFT over q in registers, the twiddle W256^(t k1), one exchange through the
-// line's scratch `xb` (16 x 17 complex; may alias the line's own input, which
-// is read before), and a 16-point DFT over t. On exit thread t holds
-// Z[t + 16 k2], the same positions as on entry. `tw` holds W_n^e at e * tws
-// (tws = 2 for a table of 512). Lanes of both lines of the warp must call it
-// together.
-template <typename T>
-__device__ __forceinline__ void fft256_h16(cplx<T> (&v)[16], int t, cplx<T>* xb, const cplx<T>* tw, int tws,
-                                           bool inv) {
+// L-point DFT in registers, L = 4, 8 or 16.
+template <typename T, int L>
+__device__ __forceinline__ void dft_small(cplx<T> (&a)[L], bool inv) {
+    if constexpr (L == 4) {
+        dft4(a[0], a[1], a[2], a[3], inv);
+    } else if constexpr (L == 8) {
+        SmallDft<T, 8>::run(a, inv, nullptr, 0);
+    } else {
+        static_assert(L == 16, "L must be 4, 8 or 16");
+        dft16(a, inv);
+    }
+}
+
+// FFT of a line of n = 16 L points held by L consecutive lanes with 16 values
+// each (the x transforms of the slab kernels at x lengths 128, 256 and 512:
+// L = 4, 8, 16; 32 / L lines per warp). Decimation in time: lane t holds
+// z[t + L q] (q = 0..15) on entry; a 16-point DFT over q in registers, the
+// twiddle W_n^(t k1), one exchange through the line's scratch `xb`
+// (16 x (L + 1) complex; may alias the line's own input, which is read
+// before), then lane t takes k1 = t + L f (f < 16 / L) and runs an L-point DFT
+// over the lanes' values of each. On exit lane t holds Z[t + L q], the same
+// positions as on entry. `tw` holds W_n^e at e * tws (tws = 2 for the table of
+// 2 n the slab kernels keep). All lanes of the warp must call it together.
+template <typename T, int L>
+__device__ __forceinline__ void fft_16xL(cplx<T> (&v)[16], int t, cplx<T>* xb, const cplx<T>* tw, int tws,
+                                         bool inv) {
+    constexpr int R = 16 / L;
     dft16(v, inv);
 #pragma unroll
     for (int k1 = 1; k1 < 16; ++k1) v[k1] = cmul(v[k1], twid(tw, t * k1, tws, inv));
     __syncwarp();
 #pragma unroll
-    for (int k1 = 0; k1 < 16; ++k1) xb[k1 * 17 + t] = v[k1];
+    for (int k1 = 0; k1 < 16; ++k1) xb[k1 * (L + 1) + t] = v[k1];
     __syncwarp();
 #pragma unroll
-    for (int j = 0; j < 16; ++j) v[j] = xb[t * 17 + j];
-    dft16(v, inv);
+    for (int f = 0; f < R; ++f) {
+        cplx<T> u[L];
+#pragma unroll
+        for (int j = 0; j < L; ++j) u[j] = xb[(t + L * f) * (L + 1) + j];
+        dft_small<T, L>(u, inv);
+#pragma unroll
+        for (int k2 = 0; k2 < L; ++k2) v[f + R * k2] = u[k2];
+    }
 }
 
-// Value of lane `src` (0..15) of this lane's 16-lane half of the warp.
-template <typename T>
-__device__ __forceinline__ cplx<T> shfl16(cplx<T> v, int src) {
-    return cplx<T>{__shfl_sync(0xffffffffu, v.x, src, 16), __shfl_sync(0xffffffffu, v.y, src, 16)};
+// Value of lane `src` (0..L-1) of this lane's L-lane segment of the warp.
+template <typename T, int L>
+__device__ __forceinline__ cplx<T> shfl_seg(cplx<T> v, int src) {
+    return cplx<T>{__shfl_sync(0xffffffffu, v.x, src, L), __shfl_sync(0xffffffffu, v.y, src, L)};
 }
 
 // Copy a twiddle table into shared memory.

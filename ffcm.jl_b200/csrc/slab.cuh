@@ -232,7 +232,7 @@ template <typename T, int BY, int BZ, int H>
 struct SpreadWin {
     static constexpr int NRP = BY * BZ;
     int key[SLAB_CAP];        // first x point of the stencil, in [0, Mx)
-    unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15)
+    unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15) | first x + 32768 (16..31)
     T y0[SLAB_CAP];
     T f[3][SLAB_CAP];
     // rows padded by one element: lanes reading different entries at the same
@@ -258,7 +258,7 @@ __device__ __forceinline__ void spread_put(const StencilParams<T>& p, SpreadWin<
                                            unsigned m, int y0r, int z0r) {
     constexpr int NRP = BY * BZ;
     W.key[i] = wrap1(sx, 2 * H);
-    W.msk[i] = m;
+    W.msk[i] = m | ((unsigned)(sx + 32768) << 16);   // the stencil's first x point, offset into bits 16..31
     W.y0[i] = y.x;
     W.f[0][i] = f.x;
     W.f[1][i] = f.y;
@@ -368,18 +368,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
                     int e = x - (int)(v >> 7);
                     if (e < 0) e += Mx;
                     const T y0 = W.y0[i];
-                    const int gx0 = (int)rint_t(mul_rn(y0, p.inv_h)) - SLAB_MG / 2;
+                    const unsigned m = W.msk[i];
+                    const int gx0 = (int)(m >> 16) - 32768;
                     T gxe, r2xe;
                     axis_weight(p, gx0 + e, y0, gxe, r2xe);
                     // (a0 + a2 (r2x + r2yz)) gx gyz = [gx (a0 + a2 r2x)] gyz + [a2 gx] [gyz r2yz]
                     const T wa = gxe * (p.a0 + p.a2 * r2xe), wc = p.a2 * gxe;
-                    const unsigned m = W.msk[i];
                     const T f0 = W.f[0][i], f1 = W.f[1][i], f2 = W.f[2][i];
+                    // rows the entry does not reach carry gyz = dyz = 0 and add nothing
 #pragma unroll
                     for (int d = 0; d < BZ; ++d)
 #pragma unroll
                         for (int b = 0; b < BY; ++b) {
-                            if (!((m >> b) & (m >> (8 + d)) & 1u)) continue;
                             const int r = d * BY + b;
                             const T wgt = wa * W.gyz[i][r] + wc * W.dyz[i][r];
                             a[0][r] += wgt * f0;
@@ -455,25 +455,28 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
         for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
         __syncthreads();
     }
-    if constexpr (H == 256 && sizeof(T) == 4) {
-        // x length 512: 16 threads per row, two rows per warp (ROWS is even,
-        // so a warp's two rows are both present or both absent); the row is
-        // its own exchange scratch; the r2c split takes Z[H - k] from the
-        // partner lane by shuffle
-        const int t = threadIdx.x & 15;
-        for (int r = (int)(threadIdx.x >> 4); r < ROWS; r += (int)(blockDim.x >> 4)) {
+    if constexpr (sizeof(T) == 4 && (H == 64 || H == 128 || H == 256)) {
+        // x lengths 128..512: L = H / 16 threads per row with 16 values each,
+        // 32 / L rows per warp (ROWS is a multiple of 32 / L, so a warp's rows
+        // are all present or all absent); the row is its own exchange scratch;
+        // the r2c split takes Z[H - k] from the partner lane by shuffle
+        constexpr int L = H / 16;
+        static_assert(ROWS % (32 / L) == 0, "a warp's rows must be all present or all absent");
+        static_assert(2 * 16 * (L + 1) <= P, "the exchange scratch must fit a slab row");
+        const int t = threadIdx.x & (L - 1);
+        for (int r = (int)(threadIdx.x / L); r < ROWS; r += (int)(blockDim.x / L)) {
             cplx<T>* rowc = reinterpret_cast<cplx<T>*>(acc + r * P);
             cplx<T> v[16];
 #pragma unroll
-            for (int q = 0; q < 16; ++q) v[q] = rowc[t + 16 * q];
-            fft256_h16(v, t, rowc, tw, 2, false);
+            for (int q = 0; q < 16; ++q) v[q] = rowc[t + L * q];
+            fft_16xL<T, L>(v, t, rowc, tw, 2, false);
             const int c = r / NRP, bd = r % NRP;
             const int b = bd % BY, d = bd / BY;
             cplx<T>* dst = spec + (((int64_t)c * p.Mz + z0r + d) * p.My + y0r + b) * hxp;
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
-                const int k = t + 16 * q;
-                const cplx<T> other = shfl16(v[15 - q], (16 - t) & 15);
+                const int k = t + L * q;
+                const cplx<T> other = shfl_seg<T, L>(v[15 - q], (L - t) & (L - 1));
                 const cplx<T> Zk = v[q];
                 const cplx<T> Zc = cconj(t == 0 ? v[(16 - q) & 15] : other);
                 const cplx<T> S = cadd(Zk, Zc), D = cmul(tw[k], csub(Zk, Zc));
@@ -577,15 +580,18 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
         mbar_wait_bounded(&bar, 0, 1 << 22);
         return;
     }
-    if constexpr (H == 256 && sizeof(T) == 4) {
-        // x length 512: 16 threads per row, two rows per warp (see the spread)
-        const int t = threadIdx.x & 15;
-        for (int r = (int)(threadIdx.x >> 4); r < ROWS; r += (int)(blockDim.x >> 4)) {
+    if constexpr (sizeof(T) == 4 && (H == 64 || H == 128 || H == 256)) {
+        // x lengths 128..512: L = H / 16 threads per row (see the spread)
+        constexpr int L = H / 16;
+        static_assert(ROWS % (32 / L) == 0, "a warp's rows must be all present or all absent");
+        static_assert(2 * 16 * (L + 1) <= P, "the exchange scratch must fit a slab row");
+        const int t = threadIdx.x & (L - 1);
+        for (int r = (int)(threadIdx.x / L); r < ROWS; r += (int)(blockDim.x / L)) {
             cplx<T>* rowc = reinterpret_cast<cplx<T>*>(acc + r * P);
             cplx<T> v[16];
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
-                const int k = t + 16 * q;
+                const int k = t + L * q;
                 cplx<T> Xk = rowc[k];
                 cplx<T> Xc = rowc[H - k];
                 if (k == 0) {
@@ -596,10 +602,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
                 const cplx<T> B = cmul(csub(Xk, cconj(Xc)), cconj(tw[k]));
                 v[q] = cadd(A, mul_pi(B));
             }
-            fft256_h16(v, t, rowc, tw, 2, true);
-            __syncwarp();   // the exchange reads of both rows are done
+            fft_16xL<T, L>(v, t, rowc, tw, 2, true);
+            __syncwarp();   // the exchange reads of the warp's rows are done
 #pragma unroll
-            for (int q = 0; q < 16; ++q) rowc[t + 16 * q] = v[q];   // real row, unpadded
+            for (int q = 0; q < 16; ++q) rowc[t + L * q] = v[q];   // real row, unpadded
         }
     } else {
     constexpr int TPL = H / 8, Q = H / 8;
