@@ -16,6 +16,11 @@ data exchange); the time is the max over ranks.
 
 --impl reference times the reference's CPU algorithm (the oracle restatement;
 the Julia reference cannot run on this machine) on the host cores.
+
+--workload selects the other measured configurations: `batched` (64
+suspensions x 16 right-hand sides in one graph launch), `adjoint` (objective
+gradient at N=100k, 256^3), `resistance` (conjugate-gradient resistance solve
+on the 512^3 system), `clustered` (N=2M in 2,000 Gaussian clusters, 1024^3).
 """
 from __future__ import annotations
 
