@@ -408,10 +408,14 @@ def run_ours(args, rank, world, local_rank):
         else:
             kept = []
             sec = cpu_baseline_run(Y, F, cpu_threads, keep=kept)
+            # the reference's default, fft_threads = 1: everything on one core
+            sec1 = cpu_baseline_run(Y, F, 1)
             cpu = {"value": N / sec, "unit": UNIT, "cores": cpu_threads, "kind": "port",
                    "sample": "one full solve of the workload by the C/pocketfft restatement of "
                              "the reference CPU path; particle loops serial as in the reference, "
-                             f"FFT on {cpu_threads} threads (fft_threads)"}
+                             f"FFT on {cpu_threads} threads (fft_threads)",
+                   "single_core": {"value": N / sec1, "unit": UNIT, "cores": 1,
+                                   "sample": "the same solve with fft_threads = 1, the reference's default"}}
             accuracy = accuracy_report(Vh.numpy(), Y, F, kept[0], cpu_threads)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
