@@ -553,40 +553,58 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
     static_assert(RB <= P * sizeof(T), "a spectrum row must fit a slab row");
     static_assert((P * sizeof(T)) % 16 == 0, "slab rows must start on 16-byte boundaries");
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bar;
+    __shared__ __align__(8) uint64_t bar[2];
+    // rows of the first transform round of the 16 x L path (256 / L); when
+    // they are fewer than the slab's, the rest arrive on a second barrier and
+    // land while the first round runs
+    constexpr bool R16 = sizeof(T) == 4 && (H == 64 || H == 128 || H == 256);
+    constexpr int R1 = R16 && 256 / (H / 16) < ROWS ? 256 / (H / 16) : ROWS;
     T* acc = reinterpret_cast<T*>(smem_raw);
     cplx<T>* dummy = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
     cplx<T>* tw = dummy + padded_len(H);   // FFT twiddles in shared memory
     load_table(tw, twx, Mx);
     const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
-    // all of the slab's spectrum rows arrive in one batch of bulk copies
-    // (row starts are 16-byte aligned: the spectrum pitch is a multiple of
-    // 128 bytes)
+    // the slab's spectrum rows arrive by bulk copies, rows [0, R1) on bar[0]
+    // and the rest on bar[1] (row starts are 16-byte aligned: the spectrum
+    // pitch is a multiple of 128 bytes)
     if (threadIdx.x == 0) {
-        mbar_init(&bar, 1);
-        mbar_arrive_expect(&bar, ROWS * RB);
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_arrive_expect(&bar[0], R1 * RB);
+        if (R1 < ROWS) mbar_arrive_expect(&bar[1], (ROWS - R1) * RB);
         for (int r = 0; r < ROWS; ++r) {
             const int c = r / NRP, bd = r % NRP;
             const cplx<T>* src = spec + (((int64_t)c * p.Mz + z0r + bd / BY) * p.My + y0r + bd % BY) * hxp;
-            bulk_load(acc + r * P, src, RB, &bar);
+            bulk_load(acc + r * P, src, RB, r < R1 ? &bar[0] : &bar[1]);
         }
     }
     __syncthreads();
-    if (!mbar_wait_bounded(&bar, 0, 1 << 22)) {
-        // the copies did not finish: report, give them one more bounded
-        // chance to land in this block's shared memory, and leave
-        if (threadIdx.x == 0) atomicOr(err, DEVERR_COPY_TIMEOUT);
-        mbar_wait_bounded(&bar, 0, 1 << 22);
-        return;
-    }
-    if constexpr (sizeof(T) == 4 && (H == 64 || H == 128 || H == 256)) {
+    // Block-uniform wait for barrier k: if the copies did not finish, report,
+    // give all of them one more bounded chance to land in this block's shared
+    // memory, and tell the caller to leave.
+    auto landed = [&](int k) -> bool {
+        const bool ok = mbar_wait_bounded(&bar[k], 0, 1 << 22);
+        if (__syncthreads_or(!ok)) {
+            if (threadIdx.x == 0) atomicOr(err, DEVERR_COPY_TIMEOUT);
+            mbar_wait_bounded(&bar[0], 0, 1 << 22);
+            if (R1 < ROWS) mbar_wait_bounded(&bar[1], 0, 1 << 22);
+            return false;
+        }
+        return true;
+    };
+    if (!landed(0)) return;
+    if constexpr (R16) {
         // x lengths 128..512: L = H / 16 threads per row (see the spread)
         constexpr int L = H / 16;
         static_assert(ROWS % (32 / L) == 0, "a warp's rows must be all present or all absent");
         static_assert(2 * 16 * (L + 1) <= P, "the exchange scratch must fit a slab row");
+        static_assert(R1 == ROWS || R1 == 256 / L, "the first round covers 256 / L rows");
         const int t = threadIdx.x & (L - 1);
-        for (int r = (int)(threadIdx.x / L); r < ROWS; r += (int)(blockDim.x / L)) {
+        for (int r0 = 0; r0 < ROWS; r0 += R1) {
+            if (r0 > 0 && !landed(1)) return;   // block-uniform
+            const int r = r0 + (int)(threadIdx.x / L);
+            if (r >= ROWS) continue;   // warp-uniform
             cplx<T>* rowc = reinterpret_cast<cplx<T>*>(acc + r * P);
             cplx<T> v[16];
 #pragma unroll
