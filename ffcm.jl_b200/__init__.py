@@ -365,6 +365,13 @@ def correct_velocities(V, config: FFCMConfig):
     return V
 
 
+def _torch_empty_particles(F, config):
+    """An (N, 3) CUDA tensor of the config's type on F's device."""
+    import torch
+    dt = torch.float32 if np.dtype(config.T) == np.float32 else torch.float64
+    return torch.empty((config.N, 3), dtype=dt, device=F.device)
+
+
 class FFCMMobility:
     """Matrix-free operator ``FFCMMobility(config, Y)`` (src/mobility.jl:374-448).
 
@@ -377,7 +384,9 @@ class FFCMMobility:
     The positions are fixed once: their cell list is built at construction
     (``ffcm_set_positions``) and every application only re-gathers the forces
     (``ffcm_mobility_apply``). If another solve ran on ``config`` in between,
-    the positions are fixed again before the application.
+    the positions are fixed again before the application. Y, and the forces
+    of ``M @ F`` / ``mul``, may be CUDA tensors: they are then used in place on
+    the current torch stream (no host staging).
     """
 
     def __init__(self, config: FFCMConfig, Y):
@@ -428,8 +437,34 @@ class FFCMMobility:
     def dtype(self):
         return np.dtype(self.config.T)
 
+    def _apply_device(self, V, F):
+        """V = M F for (N, 3) CUDA tensors of the config's type: zero copy, on
+        the current torch stream (the device fast path the reference's
+        `mul!` lacks: it stages through host arrays, src/mobility.jl:400-448)."""
+        v, f = _particle_args(self.config, (("V", V), ("F", F)), writable=("V",))
+        st = _stream_of(v)
+        lib = L_.load()
+        code = lib.ffcm_mobility_apply(self.config.handle, v.ptr, f.ptr, v.memory, st)
+        if code == L_.ERR_STATE:     # the config solved something else since
+            self._set_positions()
+            code = lib.ffcm_mobility_apply(self.config.handle, v.ptr, f.ptr, v.memory, st)
+        _raise(code)
+        return V
+
     def mul(self, v, f, alpha=None, beta=None):
         T = self.config.T
+        if _is_torch(f) and f.is_cuda:
+            out = _torch_empty_particles(f, self.config)
+            self._apply_device(out, f.reshape(self.config.N, 3).contiguous())
+            out = out.reshape(-1)
+            if alpha is None and beta is None:
+                v.copy_(out.reshape(v.shape))
+                return v
+            a = 1.0 if alpha is None else float(alpha)
+            b = 0.0 if beta is None else float(beta)
+            res = a * out if b == 0 else a * out + b * v.reshape(-1)
+            v.copy_(res.reshape(v.shape))
+            return v
         self.F_scratch[...] = np.asarray(f, T).reshape(self.config.N, 3)
         self._apply(self.V_scratch, self.F_scratch)
         out = self.V_scratch.reshape(-1)
@@ -445,6 +480,10 @@ class FFCMMobility:
         return v
 
     def __matmul__(self, F):
+        if _is_torch(F) and F.is_cuda:
+            if len(F.shape) != 2 or _julia_size(F) != (3, self.config.N):
+                raise DimensionMismatch(f"F must be 3xN for the config's N = {self.config.N}")
+            return self._apply_device(_torch_empty_particles(F, self.config), F.contiguous())
         F = np.asarray(F)
         if len(F.shape) != 2 or _julia_size(F) != (3, self.config.N):
             raise DimensionMismatch(f"F must be 3xN for the config's N = {self.config.N}")

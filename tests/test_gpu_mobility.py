@@ -340,3 +340,35 @@ def test_clustered_suspension_matches_oracle(ffcm, T):
     ffcm.mobility(V, prod, Y, F)
     err = rel_l2(V, O.apply(ora, Y, F))
     assert err < (1e-5 if T == np.float32 else 1e-10), err
+
+
+@pytest.mark.parametrize("T", TS)
+def test_fixed_position_operator_on_cuda_tensors(ffcm, T):
+    """M @ F and mul! on CUDA tensors (the zero-copy device path of
+    FFCMMobility) agree with the host-array path and with the oracle."""
+    torch = pytest.importorskip("torch")
+    N, L, M = 2000, 40.0, 64
+    cfg, ora = both(ffcm, T, **kw_of(L, N, M, R_c=3.0))
+    Y = nonoverlapping_uniform(N, (L, L, L), seed=81).astype(T)
+    F = np.random.default_rng(82).standard_normal((N, 3)).astype(T)
+    op = ffcm.FFCMMobility(cfg, Y)
+    V_host = op @ F
+    Fd = torch.from_numpy(F).cuda()
+    V_dev = op @ Fd
+    torch.cuda.synchronize()
+    bound = 2e-6 if T == np.float32 else 1e-12
+    assert rel_l2(V_dev.cpu().numpy(), V_host) < bound
+    assert rel_l2(V_dev.cpu().numpy(), O.apply(ora, Y, F)) < (1e-5 if T == np.float32 else 1e-10)
+    # mul!(v, M, f, alpha, beta) on flat 3N tensors
+    v0 = np.random.default_rng(83).standard_normal(3 * N).astype(T)
+    v_host = v0.copy()
+    op.mul(v_host, F.reshape(-1), 2.0, 0.5)
+    v_dev = torch.from_numpy(v0.copy()).cuda()
+    op.mul(v_dev, Fd.reshape(-1), 2.0, 0.5)
+    torch.cuda.synchronize()
+    assert rel_l2(v_dev.cpu().numpy(), v_host) < bound
+    # device-resident positions as well
+    op_d = ffcm.FFCMMobility(cfg, torch.from_numpy(Y).cuda())
+    V_dd = op_d @ Fd
+    torch.cuda.synchronize()
+    assert rel_l2(V_dd.cpu().numpy(), V_host) < bound
