@@ -36,7 +36,7 @@ __all__ = ["FFCMConfig", "mobility", "FFCMMobility", "FFCMBatch", "ArgumentError
            "FFCMError", "wrap_positions", "assign_cells", "sort_particles_by_cell",
            "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities",
            "mobility_checkpoint", "adjoint", "objective_gradient", "rrule_mobility",
-           "mobility_autograd", "cg", "CGHistory"]
+           "mobility_autograd", "cg", "CGHistory", "wisdom_export", "wisdom_import"]
 
 
 class ArgumentError(ValueError):
@@ -274,6 +274,14 @@ class FFCMConfig:
         _raise(L_.load().ffcm_profile_end(self.handle, ms, calls))
         return {name: (ms[i], calls[i]) for i, name in enumerate(L_.STAGES)}
 
+    def tuning(self):
+        """The y/z pass variant this configuration uses (the autotuner's, or
+        a reused / imported choice): a dict of `ffcm_get_tuning`'s fields."""
+        out = (ctypes.c_int32 * 7)()
+        _raise(L_.load().ffcm_get_tuning(self.handle, out))
+        names = ("y_kind", "y_columns", "y_grid", "z_kind", "z_columns", "z_grid", "kx_chunk")
+        return dict(zip(names, (int(x) for x in out)))
+
     def launch_count(self):
         return int(L_.load().ffcm_launch_count(self.handle))
 
@@ -499,6 +507,23 @@ class FFCMMobility:
     @staticmethod
     def isposdef():
         return True
+
+
+# ---- launch-shape wisdom (the analogue of FFTW's exported wisdom) ----
+
+def wisdom_export() -> str:
+    """The autotuner's choices of this process as text (`ffcm_wisdom_export`)."""
+    lib = L_.load()
+    n = int(lib.ffcm_wisdom_export(None, 0))
+    buf = ctypes.create_string_buffer(n + 1)
+    lib.ffcm_wisdom_export(buf, n + 1)
+    return buf.value.decode()
+
+
+def wisdom_import(text: str):
+    """Add choices from `wisdom_export` text; later configurations of those
+    shapes on this machine skip the autotuner (`ffcm_wisdom_import`)."""
+    _raise(L_.load().ffcm_wisdom_import(text.encode()))
 
 
 # ---- resistance problem: conjugate gradients on the operator ----

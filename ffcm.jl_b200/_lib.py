@@ -62,6 +62,9 @@ SIGNATURES = {
                                _i32, _i32, _i32]),
     "ffcm_destroy": (_c.c_int, [_vp]),
     "ffcm_get_info": (_c.c_int, [_vp, _i64p, _i32p, _i64p]),
+    "ffcm_get_tuning": (_c.c_int, [_vp, _i32p]),
+    "ffcm_wisdom_export": (_i64, [_c.c_char_p, _i64]),
+    "ffcm_wisdom_import": (_c.c_int, [_c.c_char_p]),
     "ffcm_mobility": (_c.c_int, [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _i64, _i32,
                                  _vp]),
     "ffcm_wrap_positions": (_c.c_int, [_vp, _vp, _i32, _vp]),

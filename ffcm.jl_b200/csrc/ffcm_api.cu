@@ -223,6 +223,22 @@ int pow2_floor(int v) {
 // ---------------------------------------------------------------------------
 // Engine: device buffers and kernels for one element type
 // ---------------------------------------------------------------------------
+// Autotuner choices per (device, element size, Mx, My, Mz), shared by all
+// configurations of the process (the y/z passes do not depend on the
+// particles), and exported / imported as text like FFTW wisdom.
+struct TunedChoice {
+    int ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk;
+};
+using TuneKey = std::array<int, 5>;
+std::mutex& tune_mu() {
+    static std::mutex m;
+    return m;
+}
+std::map<TuneKey, TunedChoice>& tune_store() {
+    static std::map<TuneKey, TunedChoice> c;
+    return c;
+}
+
 struct EngineBase {
     virtual ~EngineBase() = default;
     virtual int wrap_hash(const void* Y, bool wrap, bool hash, cudaStream_t s) = 0;
@@ -248,6 +264,9 @@ struct EngineBase {
     virtual void* adj_buf(int which) = 0;  // 0 lambda, 1 dY, 2 dF, 3 target, 4 J (double)
     virtual int ensure_real_grids() = 0;
     virtual bool uses_slab() const = 0;
+    // the y/z variant in use: ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk
+    // (-1 for an axis without the power-of-two passes)
+    virtual void tuning(int32_t* out) const = 0;
     virtual void* Y_in() = 0;
     virtual void* F_in() = 0;
     virtual void* V_out() = 0;
@@ -720,19 +739,48 @@ struct Engine final : EngineBase {
         if (v && std::sscanf(v, "%d,%d", &kind, &B) != 2) kind = B = -1;
     }
 
-    // Autotuner results per (device, precision, grid): the y/z passes do not
-    // depend on the particles, so later configurations of the same shape reuse
-    // the choice (the analogue of FFTW wisdom across configurations).
-    struct Tuned {
-        int ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk;
-    };
-    static std::mutex& tune_mu() {
-        static std::mutex m;
-        return m;
+    // True when choice t names variants this configuration can run (a
+    // stored or imported choice is used only then; the autotuner runs
+    // otherwise).
+    bool choice_valid(const TunedChoice& t) const {
+        auto in_bundles = [](int n, int B, int (*bundles)(int, int*)) {
+            int cand[4];
+            const int nc = bundles(n, cand);
+            for (int i = 0; i < nc; ++i)
+                if (cand[i] == B) return true;
+            return false;
+        };
+        if (fast_y) {
+            const int k = t.ykind, B = t.By;
+            const bool ok = (k == 0 && y_kernel<T>(My, B) && in_bundles(My, B, y_bundles)) ||
+                            (k == 1 && ypipe_kernel<T>(My, B) && hxp % B == 0 &&
+                             ypipe_smem<T>(My, B) <= 200 * 1024 && t.ygrid >= 1) ||
+                            (k == 2 && ytma_kernel<T>(My, B) && ymap_ok[log2i(B)] &&
+                             ytma_smem<T>(My, B) <= 226 * 1024 && t.ygrid >= 1);
+            if (!ok) return false;
+        }
+        if (fast_z) {
+            const int k = t.zkind, B = t.Bz;
+            const bool ok = (k == 0 && z_kernel<T>(Mz, B) && in_bundles(Mz, B, z_bundles)) ||
+                            (k == 1 && zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
+                             zpipe_smem<T>(Mz, B) <= 200 * 1024 && t.zgrid >= 1) ||
+                            (k == 2 && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= 200 * 1024) ||
+                            (k == 3 && ztma_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
+                             ztma_smem<T>(Mz, B) <= 226 * 1024 && t.zgrid >= 1);
+            if (!ok) return false;
+        }
+        const int c = t.kx_chunk;
+        return c == 0 || (fast_y && fast_z && c > 0 && c % t.By == 0 && c % t.Bz == 0 && c < nkx);
     }
-    static std::map<std::array<int, 5>, Tuned>& tune_cache() {
-        static std::map<std::array<int, 5>, Tuned> c;
-        return c;
+
+    void tuning(int32_t* out) const override {
+        out[0] = fast_y ? ykind : -1;
+        out[1] = fast_y ? By : -1;
+        out[2] = fast_y ? ygrid : -1;
+        out[3] = fast_z ? zkind : -1;
+        out[4] = fast_z ? Bz : -1;
+        out[5] = fast_z ? zgrid : -1;
+        out[6] = kx_chunk;
     }
 
     int autotune() {
@@ -743,14 +791,13 @@ struct Engine final : EngineBase {
         const bool forced = fyk >= 0 || fzk >= 0 || std::getenv("FFCM_FORCE_CHUNK") != nullptr;
         int dev = 0;
         CUDA_TRY(cudaGetDevice(&dev));
-        const std::array<int, 5> key{dev, (int)sizeof(T), Mx, My, Mz};
+        const TuneKey key{dev, (int)sizeof(T), Mx, My, Mz};
         if (!forced) {
             std::lock_guard<std::mutex> lock(tune_mu());
-            auto it = tune_cache().find(key);
-            if (it != tune_cache().end()) {
-                const Tuned& t = it->second;
-                const bool maps_ok = (t.ykind != 2 || ymap_ok[log2i(t.By)]) && (t.zkind != 3 || zmap_ok[log2i(t.Bz)]);
-                if (maps_ok) {
+            auto it = tune_store().find(key);
+            if (it != tune_store().end()) {
+                const TunedChoice& t = it->second;
+                if (choice_valid(t)) {
                     ykind = t.ykind; By = t.By; ygrid = t.ygrid;
                     zkind = t.zkind; Bz = t.Bz; zgrid = t.zgrid;
                     kx_chunk = t.kx_chunk;
@@ -860,7 +907,7 @@ struct Engine final : EngineBase {
         h->launches = 0;
         if (!forced) {
             std::lock_guard<std::mutex> lock(tune_mu());
-            tune_cache()[key] = Tuned{ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk};
+            tune_store()[key] = TunedChoice{ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk};
         }
         return FFCM_OK;
     }
@@ -1449,6 +1496,64 @@ int ffcm_destroy(ffcm_handle* h) {
     if (h->h_err) cudaFreeHost(h->h_err);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
+    return FFCM_OK;
+}
+
+int ffcm_get_tuning(const ffcm_handle* h, int32_t* out) {
+    TRY(check_handle(h));
+    if (!out) return fail(FFCM_ERR_ARGUMENT, "out must not be NULL");
+    h->eng->tuning(out);
+    return FFCM_OK;
+}
+
+int64_t ffcm_wisdom_export(char* buf, int64_t cap) {
+    std::string text;
+    {
+        std::lock_guard<std::mutex> lock(tune_mu());
+        for (const auto& kv : tune_store()) {
+            const TuneKey& k = kv.first;
+            const TunedChoice& t = kv.second;
+            char line[256];
+            std::snprintf(line, sizeof line, "ffcm-wisdom-1 %d %d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2],
+                          k[3], k[4], t.ykind, t.By, t.ygrid, t.zkind, t.Bz, t.zgrid, t.kx_chunk);
+            text += line;
+        }
+    }
+    if (buf && cap > 0) {
+        const size_t n = std::min<size_t>(text.size(), (size_t)cap - 1);
+        std::memcpy(buf, text.data(), n);
+        buf[n] = '\0';
+    }
+    return (int64_t)text.size();
+}
+
+int ffcm_wisdom_import(const char* text) {
+    g_err.clear();
+    if (!text) return fail(FFCM_ERR_ARGUMENT, "text must not be NULL");
+    std::vector<std::pair<TuneKey, TunedChoice>> parsed;
+    const char* p = text;
+    int lineno = 0;
+    while (*p) {
+        const char* e = std::strchr(p, '\n');
+        const std::string line(p, e ? (size_t)(e - p) : std::strlen(p));
+        p = e ? e + 1 : p + line.size();
+        ++lineno;
+        if (line.find_first_not_of(" \t\r") == std::string::npos) continue;   // blank line
+        int v[12];
+        char tag[32] = {0};
+        int used = 0;
+        const int got = std::sscanf(line.c_str(), "%31s %d %d %d %d %d %d %d %d %d %d %d %d %n", tag, &v[0], &v[1],
+                                    &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &v[11], &used);
+        if (got != 13 || std::strcmp(tag, "ffcm-wisdom-1") != 0 || used != (int)line.size())
+            return fail(FFCM_ERR_ARGUMENT, "wisdom line " + std::to_string(lineno) + " is malformed");
+        const bool sane = v[0] >= 0 && (v[1] == 4 || v[1] == 8) && v[2] > 0 && v[3] > 0 && v[4] > 0 && v[5] >= 0 &&
+                          v[6] > 0 && v[7] >= 0 && v[8] >= 0 && v[9] > 0 && v[10] >= 0 && v[11] >= 0;
+        if (!sane) return fail(FFCM_ERR_ARGUMENT, "wisdom line " + std::to_string(lineno) + " is out of range");
+        parsed.push_back({TuneKey{v[0], v[1], v[2], v[3], v[4]},
+                          TunedChoice{v[5], v[6], v[7], v[8], v[9], v[10], v[11]}});
+    }
+    std::lock_guard<std::mutex> lock(tune_mu());
+    for (const auto& kv : parsed) tune_store()[kv.first] = kv.second;
     return FFCM_OK;
 }
 

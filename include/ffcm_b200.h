@@ -131,6 +131,29 @@ int ffcm_destroy(ffcm_handle* h);
 /* Particle count, element type and cell count of a handle. */
 int ffcm_get_info(const ffcm_handle* h, int64_t* N, int32_t* dtype, int64_t* num_cells_total);
 
+/* ---- launch-shape wisdom --------------------------------------------------
+ * The analogue of FFTW wisdom for the reference's `fft_planning = :measure`
+ * (src/config.jl:418-423; its cost is the cold path of FFCMConfig): at
+ * ffcm_create the library times the variants of its y and z passes and keeps
+ * the fastest per (device, precision, grid); later configurations of the same
+ * shape in the process reuse it. These entry points carry the choices across
+ * processes, as FFTW's wisdom export/import does.
+ *
+ * ffcm_get_tuning: the variant a handle uses, out[7] = {y kind, y columns per
+ * tile, y grid, z kind, z columns per tile, z grid, kx chunk} (-1 for an axis
+ * without the power-of-two passes).
+ * ffcm_wisdom_export: all choices of this process as text, one line each;
+ * writes at most cap bytes including the terminating NUL into buf (buf may be
+ * NULL) and returns the full length without the NUL.
+ * ffcm_wisdom_import: adds the choices of such text (replacing those of the
+ * same key); nothing is imported from text with a malformed line
+ * (FFCM_ERR_ARGUMENT). A configuration uses an imported choice only if it
+ * names variants that configuration can run; otherwise it times them itself.
+ * The key holds the device ordinal: wisdom is for the machine that made it. */
+int ffcm_get_tuning(const ffcm_handle* h, int32_t* out);
+int64_t ffcm_wisdom_export(char* buf, int64_t cap);
+int ffcm_wisdom_import(const char* text);
+
 /* The assembled operator V = M^VF(Y) F. Replaces mobility!(V, config, Y, F)
  * (src/mobility.jl:309-331) including its staging seam
  * (ext/ForceCouplingMethodCUDAExt/mobility.jl:10-23). Shapes are Julia's
