@@ -454,17 +454,11 @@ BATCH = dict(nsys=64, nrhs=16, Nmin=2000, Nmax=64000, phi=0.1, h0=0.54, Mmin=64,
 def batched_systems():
     """64 suspensions: N log-uniform in [2k, 64k], cubic box at 10% volume
     fraction, grid the power of two nearest (in log) to L / 0.54, clamped to
-    [64, 256]."""
+    [64, 256] (tests/fixtures.py: batched_systems, shared with the tests)."""
+    from fixtures import batched_systems as make
     b = BATCH
-    rng = np.random.default_rng(b["seed"])
-    Ns = np.exp(rng.uniform(np.log(b["Nmin"]), np.log(b["Nmax"]), b["nsys"])).astype(np.int64)
-    out = []
-    for n in Ns:
-        L = float((n * 4.0 * np.pi / 3.0 / b["phi"]) ** (1.0 / 3.0))
-        M = int(2 ** int(np.round(np.log2(L / b["h0"]))))
-        M = min(b["Mmax"], max(b["Mmin"], M))
-        out.append(dict(L=(L, L, L), R_c=b["R_c"], N=int(n), num_grid_points=(M, M, M)))
-    return out
+    return make(nsys=b["nsys"], Nmin=b["Nmin"], Nmax=b["Nmax"], phi=b["phi"], h0=b["h0"], Mmin=b["Mmin"],
+                Mmax=b["Mmax"], R_c=b["R_c"], seed=b["seed"])
 
 
 def shard_systems(systems, world):
@@ -480,6 +474,41 @@ def shard_systems(systems, world):
         owner[i] = r
         load[r] += cost[i]
     return owner
+
+
+def gather_system_results(mine, parts, nsys, dist, rank):
+    """Bring every rank's per-system results to rank 0.
+
+    mine: the global indices of this rank's systems; parts: their results, in
+    the same order (any picklable values, e.g. lists of per-right-hand-side
+    arrays). Returns the list of all nsys results in global system order on
+    rank 0 (None elsewhere). With dist None (one rank) it only reorders."""
+    if dist is None:
+        out = [None] * nsys
+        for i, v in zip(mine, parts):
+            out[i] = v
+        return out
+    world = dist.get_world_size()
+    got = [None] * world
+    dist.all_gather_object(got, list(zip(mine, parts)))
+    if rank != 0:
+        return None
+    out = [None] * nsys
+    for rank_items in got:
+        for i, v in rank_items:
+            if out[i] is not None:
+                raise RuntimeError(f"system {i} was solved by two ranks")
+            out[i] = v
+    missing = [i for i, v in enumerate(out) if v is None]
+    if missing:
+        raise RuntimeError(f"systems {missing[:8]} were solved by no rank")
+    return out
+
+
+def batched_checksum(results):
+    """Checksum of checksums of the batched velocities: the float64 sum of
+    every (system, right-hand side)'s per-component sums, in system order."""
+    return float(sum(np.asarray(v, np.float64).sum() for per_sys in results for v in per_sys))
 
 
 def run_batched(args, rank, world, local_rank):
@@ -564,6 +593,12 @@ def run_batched(args, rank, world, local_rank):
         t = torch.tensor([ms_batch, ms_plain, ms_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_batch, ms_plain, ms_e2e = (float(x) for x in t)
+    # outside the timed region: every rank's velocities to rank 0, which
+    # reports a checksum of the whole batch (the same on any rank count)
+    batch.mobility(Vh, Yh, Fh, stream=stream)
+    torch.cuda.synchronize(dev)
+    per_sys = [[np.asarray(v, np.float64).sum(axis=0) for v in rhs] for rhs in batch.unpack(Vh.numpy())]
+    allres = gather_system_results(mine, per_sys, len(systems_all), dist, rank)
     if rank == 0:
         solves = b["nsys"] * b["nrhs"]
         grids = sorted(set(s["num_grid_points"][0] for s in systems_all))
@@ -587,6 +622,7 @@ def run_batched(args, rank, world, local_rank):
                     "d2h_bytes_per_step": int(Vh.numel() * 4)},
             "clocks": clk.summary(),
             "gpu_launches": int(batch.kernels_per_call * args.steps),
+            "result_checksum": batched_checksum(allres),
         }
         print(json.dumps(line), flush=True)
     batch.close()
@@ -1061,9 +1097,23 @@ def main():
         GRID = tuple(int(x) for x in args.grid.split(","))
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        # one process per GPU: start them through torch.distributed.run
+        import socket
+        import subprocess
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+               "--master-addr=127.0.0.1", f"--master-port={port}", str(Path(__file__).resolve())] + sys.argv[1:]
+        return subprocess.call(cmd)
     rank = int(os.environ.get("RANK", 0))
-    world = int(os.environ.get("WORLD_SIZE", args.gpus if args.gpus == 1 else 1))
+    world = int(os.environ.get("WORLD_SIZE", 1))
     local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    if world != args.gpus:
+        print(f"bench.py: --gpus {args.gpus} but WORLD_SIZE={world}; launch one process per GPU",
+              file=sys.stderr)
+        return 2
     if args.impl == "reference":
         return run_reference(args, rank, world)
     if args.workload == "batched":

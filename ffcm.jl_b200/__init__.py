@@ -21,8 +21,8 @@ memory; the call copies through the device and returns when V is ready) or
 CUDA ``torch.Tensor`` s of the same shape (device memory; the call is
 asynchronous on the current torch stream). Index buffers are 1-based, as in
 Julia. Errors mirror the reference: ``ArgumentError`` for invalid parameters
-(src/config.jl:288-333), ``DimensionMismatch`` for shapes
-(src/mobility.jl:315-320).
+(src/config.jl:267-312), ``DimensionMismatch`` for shapes
+(src/mobility.jl:29-34).
 """
 from __future__ import annotations
 
@@ -36,7 +36,8 @@ __all__ = ["FFCMConfig", "mobility", "FFCMMobility", "FFCMBatch", "ArgumentError
            "FFCMError", "wrap_positions", "assign_cells", "sort_particles_by_cell",
            "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities",
            "mobility_checkpoint", "adjoint", "objective_gradient", "rrule_mobility",
-           "mobility_autograd", "cg", "CGHistory", "wisdom_export", "wisdom_import"]
+           "mobility_autograd", "cg", "CGHistory", "wisdom_export", "wisdom_import", "batch_offsets",
+           "pack_batch", "unpack_batch"]
 
 
 class ArgumentError(ValueError):
@@ -99,7 +100,7 @@ def _julia_size(x):
 class _Arg:
     """A particle array handed to the C ABI (pointer, memory kind, keep-alive)."""
 
-    def __init__(self, x, T, writable=False):
+    def __init__(self, x, T, writable=False, device=None):
         self.src = x
         if _is_torch(x):
             import torch
@@ -107,6 +108,11 @@ class _Arg:
                 raise ArgumentError(f"tensor dtype {x.dtype} does not match the config's {np.dtype(T)}")
             if not x.is_contiguous():
                 raise ArgumentError("tensors must be contiguous")
+            if x.is_cuda and device is not None and x.device.index != int(device):
+                # the library's kernels run on the configuration's GPU; another
+                # GPU's memory would fault there instead of raising
+                raise ArgumentError(f"tensor lives on cuda:{x.device.index}, the configuration on "
+                                    f"cuda:{int(device)}")
             self.memory = L_.DEVICE if x.is_cuda else L_.HOST
             self.ptr = x.data_ptr()
             self.buf = x
@@ -147,7 +153,7 @@ def _stream_of(*args):
 
 
 class FFCMConfig:
-    """B200 counterpart of ``FFCMConfig{T}`` (src/config.jl:487-558).
+    """B200 counterpart of ``FFCMConfig{T}`` (src/config.jl:466-546).
 
     Validates the parameters exactly as the reference (same order, same
     ArgumentError conditions), derives the scalars in precision ``T`` and
@@ -156,11 +162,19 @@ class FFCMConfig:
     have no effect (they configure FFTW on the reference's CPU backend).
     ``gpu_acceleration`` must be true: this configuration always lives on the
     GPU; the CPU backend is the reference's own.
+
+    ``stencil_offsets`` (no reference counterpart): ``"reference"`` (default)
+    computes every stencil offset ``g h - Y`` with the reference's Float32
+    arithmetic, so results match its CPU backend to round-off;
+    ``"compensated"`` rounds the offset once at its own size
+    (``ffcm_set_stencil_offsets``), which keeps Float32 results near the
+    Float64 answer in large boxes. ``None`` keeps the library's default (the
+    ``FFCM_STENCIL_OFFSETS`` environment variable, else ``"reference"``).
     """
 
     def __init__(self, T=np.float32, *, L, R_c, N, a=1.0, kernel_widths_ratio,
                  num_grid_points, M_G, viscosity, fft_planning="measure", fft_threads=1,
-                 gpu_acceleration=True, device=0):
+                 gpu_acceleration=True, device=0, stencil_offsets=None):
         self._h = None
         self.T = np.dtype(T).type
         dt = _dtype_code(T)
@@ -200,6 +214,21 @@ class FFCMConfig:
         self.sigma, self.Sigma = T_(s.value), T_(S.value)
         self.h, self.inv_h = T_(hh.value), T_(ih.value)
         self.num_cells_total = int(np.prod(self.num_cells))
+        if stencil_offsets is not None:
+            self.stencil_offsets = stencil_offsets
+
+    @property
+    def stencil_offsets(self):
+        """``"reference"`` or ``"compensated"`` (see the class docstring)."""
+        m = ctypes.c_int32(0)
+        _raise(L_.load().ffcm_get_stencil_offsets(self.handle, ctypes.byref(m)))
+        return {v: k for k, v in L_.OFFSETS.items()}[m.value]
+
+    @stencil_offsets.setter
+    def stencil_offsets(self, mode):
+        if mode not in L_.OFFSETS:
+            raise ArgumentError(f"stencil_offsets must be 'reference' or 'compensated'; got {mode!r}")
+        _raise(L_.load().ffcm_set_stencil_offsets(self.handle, L_.OFFSETS[mode]))
 
     # -- lifetime ---------------------------------------------------------
     def close(self):
@@ -290,7 +319,7 @@ class FFCMConfig:
 
 
 def mobility(V, config: FFCMConfig, Y, F, stream=None):
-    """``mobility!(V, config, Y, F) -> V`` (src/mobility.jl:309-331).
+    """``mobility!(V, config, Y, F) -> V`` (src/mobility.jl:23-45).
 
     Overwrites V with the velocities induced by forces F at positions Y, in
     the caller's original particle order. Y and F are never modified.
@@ -303,9 +332,9 @@ def mobility(V, config: FFCMConfig, Y, F, stream=None):
         if len(getattr(x, "shape", ())) != 2:
             raise DimensionMismatch(
                 f"V, Y, and F must each be 3xN for the config's N = {config.N}")
-    v = _Arg(V, T, writable=True)
-    y = _Arg(Y, T)
-    f = _Arg(F, T)
+    v = _Arg(V, T, writable=True, device=config.device)
+    y = _Arg(Y, T, device=config.device)
+    f = _Arg(F, T, device=config.device)
     if len({v.memory, y.memory, f.memory}) != 1:
         raise ArgumentError("V, Y and F must all be host arrays or all be CUDA tensors")
     if stream is None:
@@ -321,7 +350,7 @@ def mobility(V, config: FFCMConfig, Y, F, stream=None):
 
 def wrap_positions(config: FFCMConfig, Y):
     """``wrap_positions!(config.particles.Y_wrapped, Y, config.L)``."""
-    y = _Arg(Y, config.T)
+    y = _Arg(Y, config.T, device=config.device)
     if (y.rows, y.cols) != (3, config.N):
         raise DimensionMismatch("Y must be 3xN")
     _raise(L_.load().ffcm_wrap_positions(config.handle, y.ptr, y.memory, _stream_of(y)))
@@ -336,7 +365,7 @@ def assign_cells(config: FFCMConfig):
 
 def sort_particles_by_cell(config: FFCMConfig, F):
     """``sort_particles_by_cell!(config, config.particles.Y_wrapped, F)``."""
-    f = _Arg(F, config.T)
+    f = _Arg(F, config.T, device=config.device)
     if (f.rows, f.cols) != (3, config.N):
         raise DimensionMismatch("F must be 3xN")
     _raise(L_.load().ffcm_sort_particles_by_cell(config.handle, f.ptr, f.memory, _stream_of(f)))
@@ -357,7 +386,7 @@ def stokes_solve(config: FFCMConfig):
 
 def interpolate_velocities(V, config: FFCMConfig):
     """``interpolate_velocities!(V, config)`` (overwrites V, original order)."""
-    v = _Arg(V, config.T, writable=True)
+    v = _Arg(V, config.T, writable=True, device=config.device)
     if (v.rows, v.cols) != (3, config.N):
         raise DimensionMismatch("V must be 3xN")
     _raise(L_.load().ffcm_interpolate_velocities(config.handle, v.ptr, v.memory, _stream_of(v)))
@@ -366,7 +395,7 @@ def interpolate_velocities(V, config: FFCMConfig):
 
 def correct_velocities(V, config: FFCMConfig):
     """``correct_velocities!(V, config)`` (adds to V)."""
-    v = _Arg(V, config.T, writable=True)
+    v = _Arg(V, config.T, writable=True, device=config.device)
     if (v.rows, v.cols) != (3, config.N):
         raise DimensionMismatch("V must be 3xN")
     _raise(L_.load().ffcm_correct_velocities(config.handle, v.ptr, v.memory, _stream_of(v)))
@@ -381,7 +410,7 @@ def _torch_empty_particles(F, config):
 
 
 class FFCMMobility:
-    """Matrix-free operator ``FFCMMobility(config, Y)`` (src/mobility.jl:374-448).
+    """Matrix-free operator ``FFCMMobility(config, Y)`` (src/mobility.jl:88-155).
 
     ``size`` is ``(3N, 3N)`` on the flat column-major view (entry 3(n-1)+i is
     axis i of particle n). ``mul(v, f)`` applies it, ``mul(v, f, alpha, beta)``
@@ -409,7 +438,7 @@ class FFCMMobility:
         self.config = config
         if _is_torch(Y):
             # a CUDA tensor stays on the device (a private copy: Y is never mutated)
-            self.Y = _Arg(Y, config.T).buf.detach().clone()
+            self.Y = _Arg(Y, config.T, device=config.device).buf.detach().clone()
         else:
             self.Y = np.ascontiguousarray(Y, config.T).copy()
         self.F_scratch = np.empty((config.N, 3), config.T)
@@ -417,7 +446,7 @@ class FFCMMobility:
         self._set_positions()
 
     def _set_positions(self):
-        y = _Arg(self.Y, self.config.T)
+        y = _Arg(self.Y, self.config.T, device=self.config.device)
         _raise(L_.load().ffcm_set_positions(self.config.handle, y.ptr, y.memory, _stream_of(y)))
 
     def _apply(self, V, F):
@@ -448,7 +477,7 @@ class FFCMMobility:
     def _apply_device(self, V, F):
         """V = M F for (N, 3) CUDA tensors of the config's type: zero copy, on
         the current torch stream (the device fast path the reference's
-        `mul!` lacks: it stages through host arrays, src/mobility.jl:400-448)."""
+        `mul!` lacks: it stages through host arrays, src/mobility.jl:115-147)."""
         v, f = _particle_args(self.config, (("V", V), ("F", F)), writable=("V",))
         st = _stream_of(v)
         lib = L_.load()
@@ -462,9 +491,24 @@ class FFCMMobility:
     def mul(self, v, f, alpha=None, beta=None):
         T = self.config.T
         if _is_torch(f) and f.is_cuda:
+            # the operator's element type, as the reference's mul! converts
+            # (copyto! into its T scratch, src/mobility.jl:115-147)
+            ft = f.to(_torch_empty_particles(f, self.config).dtype)
             out = _torch_empty_particles(f, self.config)
-            self._apply_device(out, f.reshape(self.config.N, 3).contiguous())
+            self._apply_device(out, ft.reshape(self.config.N, 3).contiguous())
             out = out.reshape(-1)
+            if not _is_torch(v):
+                # a host v: bring the result over and finish on the host
+                res = out.cpu().numpy()
+                vv = np.asarray(v)
+                if alpha is None and beta is None:
+                    np.copyto(vv, res.reshape(vv.shape), casting="same_kind")
+                    return v
+                a = T(1 if alpha is None else alpha)
+                b = T(0 if beta is None else beta)
+                np.copyto(vv, (a * res if b == 0 else a * res + b * vv.reshape(-1)).reshape(vv.shape),
+                          casting="same_kind")
+                return v
             if alpha is None and beta is None:
                 v.copy_(out.reshape(v.shape))
                 return v
@@ -600,7 +644,7 @@ def _particle_args(config, named, writable=()):
     for name, x in named:
         if len(getattr(x, "shape", ())) != 2:
             raise DimensionMismatch(f"{name} must be 3xN for the config's N = {config.N}")
-        a = _Arg(x, T, writable=name in writable)
+        a = _Arg(x, T, writable=name in writable, device=config.device)
         if (a.rows, a.cols) != (3, config.N):
             raise DimensionMismatch(f"{name} must be 3xN for the config's N = {config.N}; "
                                     f"got size ({a.rows}, {a.cols})")
@@ -737,6 +781,36 @@ def derive_scalars(T, *, L, R_c, a=1.0, kernel_widths_ratio, num_grid_points):
                 h=T_(hh.value), inv_h=T_(ih.value))
 
 
+def batch_offsets(Ns, nrhs):
+    """Row offsets of the batched layout (``ffcm_batch_create``): system i's
+    positions start at row ``yoff[i]`` of the ``(sum N, 3)`` position array,
+    its right-hand side r at row ``fvoff[i] + r * N[i]`` of the
+    ``(nrhs * sum N, 3)`` force and velocity arrays."""
+    Ns = np.asarray(Ns, np.int64)
+    yoff = np.concatenate([[0], np.cumsum(Ns)[:-1]]).astype(np.int64)
+    return yoff, int(nrhs) * yoff
+
+
+def pack_batch(T, Ys=None, Fs=None):
+    """Flatten per-system positions [(N_i, 3)] and forces [[(N_i, 3)] * nrhs]
+    into the batched layout (host arrays of type T)."""
+    out = []
+    if Ys is not None:
+        out.append(np.ascontiguousarray(np.concatenate([np.asarray(y, T).reshape(-1, 3) for y in Ys]), T))
+    if Fs is not None:
+        out.append(np.ascontiguousarray(np.concatenate(
+            [np.asarray(f, T).reshape(-1, 3) for fr in Fs for f in fr]), T))
+    return out[0] if len(out) == 1 else tuple(out)
+
+
+def unpack_batch(V, Ns, nrhs):
+    """Split a batched velocity array into [[(N_i, 3)] * nrhs] per system (views)."""
+    V = np.asarray(V)
+    _, fvoff = batch_offsets(Ns, nrhs)
+    return [[V[fvoff[i] + r * n: fvoff[i] + (r + 1) * n] for r in range(int(nrhs))]
+            for i, n in enumerate(int(x) for x in Ns)]
+
+
 class FFCMBatch:
     """Batched form: ``nsys`` independent suspensions, each with ``nrhs`` force
     right-hand sides, solved by one CUDA-graph launch per call.
@@ -768,11 +842,11 @@ class FFCMBatch:
             float(kernel_widths_ratio), _i32ptr(Ms), int(M_G), float(viscosity), int(nrhs),
             int(device)))
         self._b = b
+        self.device = int(device)
         self.N = Ns
         self.nrhs = int(nrhs)
         self.nsys = n
-        self.yoff = np.concatenate([[0], np.cumsum(Ns)[:-1]]).astype(np.int64)
-        self.fvoff = self.nrhs * self.yoff
+        self.yoff, self.fvoff = batch_offsets(Ns, self.nrhs)
         total, ns, nr, kern = (ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int32(),
                                ctypes.c_int64())
         _raise(L_.load().ffcm_batch_get_info(b, ctypes.byref(total), ctypes.byref(ns),
@@ -793,27 +867,18 @@ class FFCMBatch:
 
     def pack(self, Ys=None, Fs=None):
         """Flatten per-system positions [(N_i,3)] and forces [[(N_i,3)] * nrhs]."""
-        out = []
-        if Ys is not None:
-            out.append(np.ascontiguousarray(np.concatenate(
-                [np.asarray(y, self.T).reshape(-1, 3) for y in Ys]), self.T))
-        if Fs is not None:
-            out.append(np.ascontiguousarray(np.concatenate(
-                [np.asarray(f, self.T).reshape(-1, 3) for fr in Fs for f in fr]), self.T))
-        return out[0] if len(out) == 1 else tuple(out)
+        return pack_batch(self.T, Ys, Fs)
 
     def unpack(self, V):
         """Split a flat velocity array into [[(N_i,3)] * nrhs] per system."""
-        V = np.asarray(V)
-        return [[V[self.fvoff[i] + r * n: self.fvoff[i] + (r + 1) * n] for r in range(self.nrhs)]
-                for i, n in enumerate(self.N)]
+        return unpack_batch(V, self.N, self.nrhs)
 
     def mobility(self, V, Y, F, stream=None):
         T = self.T
         tot = self.total_particles
-        v = _Arg(V, T, writable=True)
-        y = _Arg(Y, T)
-        f = _Arg(F, T)
+        v = _Arg(V, T, writable=True, device=self.device)
+        y = _Arg(Y, T, device=self.device)
+        f = _Arg(F, T, device=self.device)
         if (y.rows, y.cols) != (3, tot) or (f.rows, f.cols) != (3, tot * self.nrhs) or \
                 (v.rows, v.cols) != (3, tot * self.nrhs):
             raise DimensionMismatch("batch arrays must be (sum N, 3) for Y and "

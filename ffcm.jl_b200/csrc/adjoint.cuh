@@ -77,8 +77,9 @@ __global__ void k_adjoint_gather(int n_part, const vec4<T>* __restrict__ Ys, con
             const int gi = j + (k - p.half);
             // one rounding (fused multiply-add) instead of the forward's two:
             // the gradient sums cancel strongly, so the offset's accuracy
-            // matters more here than in the forward
-            const T x = fma_t((T)gi, p.h, -yy);
+            // matters more here than in the forward; with compensated offsets
+            // the forward's own (more accurate) offset
+            const T x = p.comp ? stencil_offset(p, gi, yy) : fma_t((T)gi, p.h, -yy);
             g[e] = p.inv_norm * exp_t(-x * x * p.inv_2S2);
             xo[e] = x;
             idx[e] = imod(gi, M);

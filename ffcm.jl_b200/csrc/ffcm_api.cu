@@ -9,6 +9,7 @@
 #include <cstring>
 #include <cstdlib>
 #include <functional>
+#include <initializer_list>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -111,7 +112,7 @@ struct DeviceGuard {
 };
 
 // ---------------------------------------------------------------------------
-// Cold path, in the working precision T (src/config.jl:288-380)
+// Cold path, in the working precision T (src/config.jl:267-359)
 // ---------------------------------------------------------------------------
 template <typename T>
 struct Derived {
@@ -223,13 +224,15 @@ int pow2_floor(int v) {
 // ---------------------------------------------------------------------------
 // Engine: device buffers and kernels for one element type
 // ---------------------------------------------------------------------------
-// Autotuner choices per (device, element size, Mx, My, Mz), shared by all
-// configurations of the process (the y/z passes do not depend on the
-// particles), and exported / imported as text like FFTW wisdom.
+// Autotuner choices per (device ordinal, element size, Mx, My, Mz, SM count),
+// shared by all configurations of the process (the y/z passes do not depend
+// on the particles), and exported / imported as text like FFTW wisdom. The SM
+// count keeps a choice made on one GPU model from being applied to another
+// that happens to have the same ordinal.
 struct TunedChoice {
     int ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk;
 };
-using TuneKey = std::array<int, 5>;
+using TuneKey = std::array<int, 6>;
 std::mutex& tune_mu() {
     static std::mutex m;
     return m;
@@ -264,6 +267,8 @@ struct EngineBase {
     virtual void* adj_buf(int which) = 0;  // 0 lambda, 1 dY, 2 dF, 3 target, 4 J (double)
     virtual int ensure_real_grids() = 0;
     virtual bool uses_slab() const = 0;
+    // stencil offset arithmetic of every later launch (FFCM_OFFSETS_*)
+    virtual void set_offsets(int mode) = 0;
     // the y/z variant in use: ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk
     // (-1 for an axis without the power-of-two passes)
     virtual void tuning(int32_t* out) const = 0;
@@ -289,6 +294,7 @@ struct ffcm_handle {
     int64_t N = 0;
     int32_t M[3] = {0, 0, 0};
     int32_t M_G = 0;
+    int32_t offsets = FFCM_OFFSETS_REFERENCE;   // stencil offset arithmetic
     int32_t num_cells[3] = {0, 0, 0};
     int64_t ncell = 0;
     size_t esize = 4;
@@ -456,7 +462,7 @@ struct Engine final : EngineBase {
         plane = (int64_t)Mx * My * Mz;
         const T mu = T(mu_d);
 
-        // stencil scalars (src/stencil.jl:311-320)
+        // stencil scalars (src/stencil.jl:22-31)
         const T S2 = d.Sigma * d.Sigma;
         const T S4 = S2 * S2;
         const T dd = d.sigma * d.sigma - S2;
@@ -466,6 +472,9 @@ struct Engine final : EngineBase {
         sp.a2 = dd / (T(2) * S4);
         sp.inv_norm = T(1) / std::sqrt(T(2) * T(kPi) * S2);
         sp.inv_2S2 = T(1) / (T(2) * S2);
+        // rounding error of h against the exact spacing of the box in T
+        sp.h_lo = T((long double)L[0] / (long double)Mx - (long double)d.h);
+        sp.comp = h->offsets == FFCM_OFFSETS_COMPENSATED ? 1 : 0;
         h3 = d.h * d.h * d.h;
         const T inv_M = T(1) / T((double)plane);
         inv_mu_M = inv_M / mu;
@@ -628,7 +637,7 @@ struct Engine final : EngineBase {
             TRY(alloc(slab_counts, (size_t)sg.nty * sg.ntz));
         }
 
-        // zero-initialised grids and cell list (src/config.jl:464-469)
+        // zero-initialised grids and cell list (src/config.jl:443-448)
         CUDA_TRY(cudaMemset(spec, 0, 3 * (size_t)hxp * My * Mz * sizeof(cplx<T>)));
         if (fast_z || fast_y) make_tma_maps();
         CUDA_TRY(cudaMemset(off, 0, ((size_t)ncell + 1) * sizeof(int32_t)));
@@ -652,7 +661,7 @@ struct Engine final : EngineBase {
         TRY(table(My, twy));
         TRY(table(Mz, twz));
 
-        // wavevectors (src/config.jl:254-258, 374-377), in T
+        // wavevectors (src/config.jl:233-237, 353-356), in T
         const T twopi = T(2) * T(kPi);
         std::vector<T> kx(nkx), ky(My), kz(Mz);
         for (int i = 0; i < nkx; ++i) kx[i] = twopi * T(i) / L[0];
@@ -769,6 +778,10 @@ struct Engine final : EngineBase {
                              ztma_smem<T>(Mz, B) <= 226 * 1024 && t.zgrid >= 1);
             if (!ok) return false;
         }
+        // persistent grids are at most (blocks per SM) x SMs; anything larger
+        // came from elsewhere and would launch far too many blocks
+        const int gmax = 64 * num_sms;
+        if ((fast_y && t.ygrid > gmax) || (fast_z && t.zgrid > gmax)) return false;
         const int c = t.kx_chunk;
         return c == 0 || (fast_y && fast_z && c > 0 && c % t.By == 0 && c % t.Bz == 0 && c < nkx);
     }
@@ -791,7 +804,7 @@ struct Engine final : EngineBase {
         const bool forced = fyk >= 0 || fzk >= 0 || std::getenv("FFCM_FORCE_CHUNK") != nullptr;
         int dev = 0;
         CUDA_TRY(cudaGetDevice(&dev));
-        const TuneKey key{dev, (int)sizeof(T), Mx, My, Mz};
+        const TuneKey key{dev, (int)sizeof(T), Mx, My, Mz, num_sms};
         if (!forced) {
             std::lock_guard<std::mutex> lock(tune_mu());
             auto it = tune_store().find(key);
@@ -926,6 +939,7 @@ struct Engine final : EngineBase {
     }
 
     bool uses_slab() const override { return slab; }
+    void set_offsets(int mode) override { sp.comp = mode == FFCM_OFFSETS_COMPENSATED ? 1 : 0; }
 
     int gather_forces(const void* F, cudaStream_t s) override {
         StageScope sc(h, FFCM_STAGE_CELL_LIST, s);
@@ -1288,6 +1302,36 @@ int check_memory(int32_t memory) {
     return FFCM_OK;
 }
 
+// FFCM_DEVICE arguments are read and written by kernels launched on `device`.
+// Memory of another GPU, or a host pointer that CUDA does not know, would
+// fault there instead of failing the call, so both are rejected up front.
+// Pinned (registered) host memory and managed memory are reachable from every
+// GPU and pass. NULL entries are skipped (the callers check them).
+int check_device_ptrs(int device, std::initializer_list<const void*> ptrs) {
+    for (const void* p : ptrs) {
+        if (!p) continue;
+        cudaPointerAttributes a{};
+        const cudaError_t e = cudaPointerGetAttributes(&a, p);
+        if (e != cudaSuccess) {
+            cudaGetLastError();   // clear the non-sticky error
+            return fail(FFCM_ERR_ARGUMENT, std::string("an FFCM_DEVICE pointer is not CUDA memory: ") +
+                                               cudaGetErrorString(e));
+        }
+        if (a.type == cudaMemoryTypeUnregistered)
+            return fail(FFCM_ERR_ARGUMENT, "an FFCM_DEVICE pointer is ordinary host memory; pass FFCM_HOST");
+        if (a.type == cudaMemoryTypeDevice && a.device != device)
+            return fail(FFCM_ERR_ARGUMENT, "an FFCM_DEVICE pointer lives on GPU " + std::to_string(a.device) +
+                                               ", the configuration on GPU " + std::to_string(device));
+    }
+    return FFCM_OK;
+}
+
+// check_memory, then (device memory only) check_device_ptrs.
+int check_args(int device, int32_t memory, std::initializer_list<const void*> ptrs) {
+    TRY(check_memory(memory));
+    return memory == FFCM_DEVICE ? check_device_ptrs(device, ptrs) : FFCM_OK;
+}
+
 // Synchronise and surface sticky device-side errors.
 int finish(ffcm_handle* h, cudaStream_t s) {
     CUDA_TRY(cudaMemcpyAsync(h->h_err, h->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
@@ -1469,6 +1513,12 @@ int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, i
     for (int i = 0; i < 3; ++i) h->M[i] = M[i];
     h->M_G = M_G;
     h->esize = dtype == FFCM_FLOAT32 ? 4 : 8;
+    {
+        const char* v = std::getenv("FFCM_STENCIL_OFFSETS");
+        if (v && std::strcmp(v, "compensated") == 0) h->offsets = FFCM_OFFSETS_COMPENSATED;
+        else if (v && *v && std::strcmp(v, "reference") != 0)
+            return fail(FFCM_ERR_ARGUMENT, "FFCM_STENCIL_OFFSETS must be \"reference\" or \"compensated\"");
+    }
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMalloc(&h->d_err, sizeof(int)));
     CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(int)));
@@ -1514,8 +1564,8 @@ int64_t ffcm_wisdom_export(char* buf, int64_t cap) {
             const TuneKey& k = kv.first;
             const TunedChoice& t = kv.second;
             char line[256];
-            std::snprintf(line, sizeof line, "ffcm-wisdom-1 %d %d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1], k[2],
-                          k[3], k[4], t.ykind, t.By, t.ygrid, t.zkind, t.Bz, t.zgrid, t.kx_chunk);
+            std::snprintf(line, sizeof line, "ffcm-wisdom-2 %d %d %d %d %d %d %d %d %d %d %d %d %d\n", k[0], k[1],
+                          k[2], k[3], k[4], k[5], t.ykind, t.By, t.ygrid, t.zkind, t.Bz, t.zgrid, t.kx_chunk);
             text += line;
         }
     }
@@ -1539,21 +1589,50 @@ int ffcm_wisdom_import(const char* text) {
         p = e ? e + 1 : p + line.size();
         ++lineno;
         if (line.find_first_not_of(" \t\r") == std::string::npos) continue;   // blank line
-        int v[12];
+        int v[13];
         char tag[32] = {0};
         int used = 0;
-        const int got = std::sscanf(line.c_str(), "%31s %d %d %d %d %d %d %d %d %d %d %d %d %n", tag, &v[0], &v[1],
-                                    &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &v[11], &used);
-        if (got != 13 || std::strcmp(tag, "ffcm-wisdom-1") != 0 || used != (int)line.size())
+        const int got = std::sscanf(line.c_str(), "%31s %d %d %d %d %d %d %d %d %d %d %d %d %d %n", tag, &v[0],
+                                    &v[1], &v[2], &v[3], &v[4], &v[5], &v[6], &v[7], &v[8], &v[9], &v[10], &v[11],
+                                    &v[12], &used);
+        if (got != 14 || std::strcmp(tag, "ffcm-wisdom-2") != 0 || used != (int)line.size())
             return fail(FFCM_ERR_ARGUMENT, "wisdom line " + std::to_string(lineno) + " is malformed");
-        const bool sane = v[0] >= 0 && (v[1] == 4 || v[1] == 8) && v[2] > 0 && v[3] > 0 && v[4] > 0 && v[5] >= 0 &&
-                          v[6] > 0 && v[7] >= 0 && v[8] >= 0 && v[9] > 0 && v[10] >= 0 && v[11] >= 0;
+        // grid sizes and SM counts far beyond any GPU are rejected here;
+        // choice_valid bounds the grids again against the device in use
+        const bool sane = v[0] >= 0 && (v[1] == 4 || v[1] == 8) && v[2] > 0 && v[3] > 0 && v[4] > 0 && v[5] > 0 &&
+                          v[5] <= 4096 && v[6] >= 0 && v[7] > 0 && v[8] >= 0 && v[8] <= (1 << 18) && v[9] >= 0 &&
+                          v[10] > 0 && v[11] >= 0 && v[11] <= (1 << 18) && v[12] >= 0;
         if (!sane) return fail(FFCM_ERR_ARGUMENT, "wisdom line " + std::to_string(lineno) + " is out of range");
-        parsed.push_back({TuneKey{v[0], v[1], v[2], v[3], v[4]},
-                          TunedChoice{v[5], v[6], v[7], v[8], v[9], v[10], v[11]}});
+        parsed.push_back({TuneKey{v[0], v[1], v[2], v[3], v[4], v[5]},
+                          TunedChoice{v[6], v[7], v[8], v[9], v[10], v[11], v[12]}});
     }
     std::lock_guard<std::mutex> lock(tune_mu());
     for (const auto& kv : parsed) tune_store()[kv.first] = kv.second;
+    return FFCM_OK;
+}
+
+int ffcm_set_stencil_offsets(ffcm_handle* h, int32_t mode) {
+    g_err.clear();
+    TRY(check_handle(h));
+    if (mode != FFCM_OFFSETS_REFERENCE && mode != FFCM_OFFSETS_COMPENSATED)
+        return fail(FFCM_ERR_ARGUMENT, "mode must be FFCM_OFFSETS_REFERENCE or FFCM_OFFSETS_COMPENSATED");
+    if (mode == h->offsets) return FFCM_OK;
+    DeviceGuard g(h->device);
+    // work already queued keeps the mode it was launched with
+    if (h->stream) CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->offsets = mode;
+    h->eng->set_offsets(mode);
+    // a checkpoint was made with the other weights, and the conjugate-gradient
+    // graph holds the old kernel parameters: neither may be reused
+    h->ckpt = false;
+    cg_release(h);
+    return FFCM_OK;
+}
+
+int ffcm_get_stencil_offsets(const ffcm_handle* h, int32_t* mode) {
+    TRY(check_handle(h));
+    if (!mode) return fail(FFCM_ERR_ARGUMENT, "mode must not be NULL");
+    *mode = h->offsets;
     return FFCM_OK;
 }
 
@@ -1572,7 +1651,7 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
     TRY(check_handle(h));
     h->ckpt = false;
     h->positions = false;
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {V, Y, F}));
     const int64_t N = h->N;
     if (!(vr == 3 && vc == N && yr == 3 && yc == N && fr == 3 && fc == N)) {
         return fail(FFCM_ERR_DIMENSION,
@@ -1615,7 +1694,7 @@ int ffcm_wrap_positions(ffcm_handle* h, const void* Y, int32_t memory, void* str
     TRY(check_handle(h));
     h->ckpt = false;
     h->positions = false;
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {Y}));
     if (!Y) return fail(FFCM_ERR_ARGUMENT, "Y must not be NULL");
     DeviceGuard g(h->device);
     cudaStream_t s = h->pick(stream);
@@ -1643,7 +1722,7 @@ int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, v
     TRY(check_handle(h));
     h->ckpt = false;
     h->positions = false;
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {F}));
     if (!F) return fail(FFCM_ERR_ARGUMENT, "F must not be NULL");
     DeviceGuard g(h->device);
     cudaStream_t s = h->pick(stream);
@@ -1678,7 +1757,7 @@ int ffcm_stokes_solve(ffcm_handle* h, void* stream) {
 int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {V}));
     if (!V) return fail(FFCM_ERR_ARGUMENT, "V must not be NULL");
     DeviceGuard g(h->device);
     cudaStream_t s = h->pick(stream);
@@ -1692,7 +1771,7 @@ int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* s
 int ffcm_correct_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {V}));
     if (!V) return fail(FFCM_ERR_ARGUMENT, "V must not be NULL");
     DeviceGuard g(h->device);
     cudaStream_t s = h->pick(stream);
@@ -1708,7 +1787,7 @@ int ffcm_mobility_checkpoint(ffcm_handle* h, void* V, const void* Y, const void*
                              void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {V, Y, F}));
     h->ckpt = false;
     h->positions = false;
     if (!V || !Y || !F) return fail(FFCM_ERR_ARGUMENT, "V, Y and F must not be NULL");
@@ -1747,7 +1826,7 @@ int ffcm_mobility_checkpoint(ffcm_handle* h, void* V, const void* Y, const void*
 int ffcm_adjoint(ffcm_handle* h, void* dJdY, void* dJdF, const void* lambda, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {dJdY, dJdF, lambda}));
     if (!dJdY || !dJdF || !lambda) return fail(FFCM_ERR_ARGUMENT, "dJdY, dJdF and lambda must not be NULL");
     if (!h->ckpt)
         return fail(FFCM_ERR_STATE,
@@ -1775,7 +1854,7 @@ int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, v
                             const void* F, const void* V_target, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {J, dJdY, dJdF, V, Y, F, V_target}));
     h->ckpt = false;
     h->positions = false;
     if (!J || !dJdY || !dJdF || !V || !Y || !F || !V_target)
@@ -1825,7 +1904,7 @@ int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, v
 int ffcm_set_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {Y}));
     h->ckpt = false;
     h->positions = false;
     if (!Y) return fail(FFCM_ERR_ARGUMENT, "Y must not be NULL");
@@ -1852,7 +1931,7 @@ int ffcm_set_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stre
 int ffcm_mobility_apply(ffcm_handle* h, void* V, const void* F, int32_t memory, void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {V, F}));
     if (!V || !F) return fail(FFCM_ERR_ARGUMENT, "V and F must not be NULL");
     if (!h->positions)
         return fail(FFCM_ERR_STATE,
@@ -1887,7 +1966,7 @@ int ffcm_cg_solve(ffcm_handle* h, void* F, const void* V, int32_t memory, double
                   void* stream) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {F, V}));
     if (!F || !V) return fail(FFCM_ERR_ARGUMENT, "F and V must not be NULL");
     if (flags & ~FFCM_CG_INITIAL_GUESS) return fail(FFCM_ERR_ARGUMENT, "unknown flag bits");
     if (!(abstol >= 0) || std::isnan(reltol) || std::isinf(reltol) || std::isinf(abstol))
@@ -2059,7 +2138,7 @@ int buffer_dispatch(ffcm_handle* h, int32_t which, void* ext, int64_t nbytes, in
                     void* stream, bool get) {
     g_err.clear();
     TRY(check_handle(h));
-    TRY(check_memory(memory));
+    TRY(check_args(h->device, memory, {ext}));
     if (!ext) return fail(FFCM_ERR_ARGUMENT, "buffer pointer must not be NULL");
     DeviceGuard g(h->device);
     cudaStream_t s = h->pick(stream);
@@ -2309,7 +2388,7 @@ int ffcm_batch_mobility(ffcm_batch* b, void* V, const void* Y, const void* F, in
                         void* stream) {
     g_err.clear();
     if (!b || !b->exec) return fail(FFCM_ERR_STATE, "null or unbuilt batch");
-    TRY(check_memory(memory));
+    TRY(check_args(b->device, memory, {V, Y, F}));
     if (!V || !Y || !F) return fail(FFCM_ERR_ARGUMENT, "V, Y and F must not be NULL");
     DeviceGuard g(b->device);
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : b->main;
@@ -2350,9 +2429,10 @@ int ffcm_batch_mobility(ffcm_batch* b, void* V, const void* Y, const void* F, in
 //   * the scratch is one array per device: calls that overlap in time on one
 //     device (different streams, different host threads) race on it and must
 //     be serialised by the caller;
-//   * the first call on each device looks the scratch up with
-//     cudaGetSymbolAddress (which may load this library's device code onto
-//     that device); make that first call before any stream capture begins;
+//   * every call looks the scratch up with cudaGetSymbolAddress on the
+//     current device; the first call on a device may load this library's
+//     device code there, so make that first call before any stream capture
+//     begins (a reset device reloads it on the next call);
 //   * nothing needs to be zero beforehand: every call clears the counters it
 //     uses and its range-check flag before counting;
 //   * the call runs on the calling thread's current device, on `stream`, and
@@ -2373,22 +2453,16 @@ static __device__ __align__(256) int32_t g_noalloc_scratch[kNoallocScratchInts];
 
 namespace {
 
-std::mutex g_noalloc_mu;
-int32_t* g_noalloc_ptr[64] = {};
-
-// Resolve (once per device) the device address of the scratch array.
+// The device address of the scratch array on the current device. It is looked
+// up on every call, not cached: cudaGetSymbolAddress of an already loaded
+// module is a table lookup with no device work, and a cached address would go
+// stale if the caller reset the device (cudaDeviceReset unloads the module;
+// the next lookup loads it again at a possibly different address).
 int noalloc_scratch(int32_t** out) {
-    int dev = 0;
-    CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return fail(FFCM_ERR_UNSUPPORTED, "device ordinal above 63");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(cell-sort scratch)");
-        g_noalloc_ptr[dev] = static_cast<int32_t*>(p);
-    }
-    *out = g_noalloc_ptr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(cell-sort scratch)");
+    *out = static_cast<int32_t*>(p);
     return FFCM_OK;
 }
 
@@ -2454,6 +2528,9 @@ extern "C" int ffcm_sort_cells_noalloc(const int32_t* cell_hash, int64_t N, int3
                                            "] (the fixed scratch size); got " + std::to_string(ncell));
     if ((N > 0 && (!cell_hash || !original_index)) || !cell_start || !cell_end)
         return fail(FFCM_ERR_ARGUMENT, "cell_hash, original_index, cell_start and cell_end must not be NULL");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    TRY(check_device_ptrs(dev, {cell_hash, original_index, cell_start, cell_end}));
     int32_t* scratch = nullptr;
     TRY(noalloc_scratch(&scratch));
     cudaStream_t s = static_cast<cudaStream_t>(stream);

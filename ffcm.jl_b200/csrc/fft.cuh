@@ -4,7 +4,7 @@
 //
 //   x r2c  ->  y fwd  ->  [z fwd, projector, z inv]  ->  y inv  ->  x c2r
 //
-// Reference: src/stokes_solve.jl:151-172 (unnormalised FFTW r2c / c2r; the
+// Reference: src/stokes_solve.jl:21-42 (unnormalised FFTW r2c / c2r; the
 // 1/M normalisation folded into the projector) and :200-240 (the projector
 // f <- (inv_M/mu)(1/k^2)(f - k (k.f)/k^2), k = 0 -> 0). The c2r follows the
 // FFTW / pocketfft convention for the halved x axis: complex inverse DFTs over

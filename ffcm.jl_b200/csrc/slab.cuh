@@ -19,7 +19,7 @@
 //    straight to the spectrum.
 //  * k_interp_slab: the slab's spectrum rows are x-c2r transformed into shared
 //    memory; one thread per listed particle gathers its partial velocity over
-//    the slab rows from registers (src/interpolate.jl:322-376) and adds it,
+//    the slab rows from registers (src/interpolate.jl:82-136) and adds it,
 //    with an L2 reduction, to a sorted-order velocity buffer that the
 //    correction kernel finishes (h^3 scale, correction, scatter to the
 //    caller's order).
@@ -153,10 +153,10 @@ __device__ __forceinline__ void slab_anchor(const StencilParams<T>& p, const vec
 }
 
 // Gaussian factor and squared offset of stencil point g along one axis, with
-// the reference's x = g h - Y (src/stencil.jl:80-112).
+// the reference's x = g h - Y (src/stencil.jl:80-112; stencil_offset).
 template <typename T>
 __device__ __forceinline__ void axis_weight(const StencilParams<T>& p, int g, T y, T& gw, T& r2) {
-    const T x = sub_rn(mul_rn((T)g, p.h), y);
+    const T x = stencil_offset(p, g, y);
     r2 = mul_rn(x, x);
     gw = p.inv_norm * exp_t(-r2 * p.inv_2S2);
 }

@@ -18,7 +18,28 @@ template <typename T>
 struct StencilParams {
     int Mx, My, Mz, MG, half;
     T h, inv_h, a0, a2, inv_norm, inv_2S2;
+    // compensated stencil offsets (opt-in): h_lo is the rounding error of h
+    // against the exact spacing L / M of the configuration's box
+    T h_lo;
+    int comp;
 };
+
+// Offset x = g h - y of stencil point g from a particle at y.
+//  * reference arithmetic (comp = 0; src/stencil.jl:105, `T.(g) .* h .- Y`):
+//    the product g h is rounded to T before the subtraction. When g h and y
+//    are both near the box length L the difference keeps only the bits the
+//    two roundings leave, an absolute error of order ulp(L) (3e-5 at
+//    L = 275.6 in Float32) in every Gaussian weight;
+//  * compensated (comp = 1): h = h + h_lo as a two-term split of the exact
+//    spacing, x = fma(g, h, -y) + g h_lo, so x is rounded once at its own
+//    size (~M_G h / 2): the Float32 result then sits within the Float64
+//    answer's 1e-5 instead of 2e-4 at that box size. Bit parity with the
+//    reference's Float32 arithmetic is given up, so this is not the default.
+template <typename T>
+__device__ __forceinline__ T stencil_offset(const StencilParams<T>& p, int g, T y) {
+    if (p.comp) return fma_t((T)g, p.h, -y) + (T)g * p.h_lo;
+    return sub_rn(mul_rn((T)g, p.h), y);
+}
 
 // Per-warp shared stencil: g[3][MG], r2[3][MG], idx[3][MG].
 template <typename T>
@@ -39,7 +60,7 @@ __device__ __forceinline__ void fill_stencil_warp(const StencilParams<T>& p, T y
         int M = axis == 0 ? p.Mx : (axis == 1 ? p.My : p.Mz);
         int j = (int)rint_t(mul_rn(y, p.inv_h));
         int g = j + (k - p.half);
-        T x = sub_rn(mul_rn((T)g, p.h), y);
+        T x = stencil_offset(p, g, y);
         T x2 = mul_rn(x, x);
         st.g[e] = p.inv_norm * exp_t(-x2 * p.inv_2S2);
         st.r2[e] = x2;

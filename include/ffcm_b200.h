@@ -25,7 +25,7 @@
  *    1-based, as in the reference (`original_index`, `cell_start`,
  *    `cell_end`); cell hashes are 0-based as in the reference.
  *  - A handle is not re-entrant: one host thread at a time, as the reference
- *    FFCMConfig (src/config.jl:155-160).
+ *    FFCMConfig (src/config.jl:196-215).
  */
 #ifndef FFCM_B200_H
 #define FFCM_B200_H
@@ -38,8 +38,8 @@ extern "C" {
 
 /* ---- status codes ------------------------------------------------------- */
 #define FFCM_OK 0
-#define FFCM_ERR_ARGUMENT 1    /* Julia ArgumentError (src/config.jl:288-333)      */
-#define FFCM_ERR_DIMENSION 2   /* Julia DimensionMismatch (src/mobility.jl:315-320) */
+#define FFCM_ERR_ARGUMENT 1    /* Julia ArgumentError (src/config.jl:267-312)      */
+#define FFCM_ERR_DIMENSION 2   /* Julia DimensionMismatch (src/mobility.jl:29-34) */
 #define FFCM_ERR_OOM 3         /* device or host allocation failed                 */
 #define FFCM_ERR_CUDA 4        /* CUDA runtime error                                */
 #define FFCM_ERR_TIMEOUT 5     /* a bounded device-side wait gave up                */
@@ -50,7 +50,7 @@ extern "C" {
 #define FFCM_FLOAT32 0
 #define FFCM_FLOAT64 1
 
-/* ---- fft_planning (src/config.jl:189-193); accepted and validated only ---- */
+/* ---- fft_planning (src/config.jl:168-172); accepted and validated only ---- */
 #define FFCM_FFT_ESTIMATE 0
 #define FFCM_FFT_MEASURE 1
 #define FFCM_FFT_PATIENT 2
@@ -61,16 +61,16 @@ extern "C" {
 
 /* ---- buffers reachable by ffcm_get_buffer / ffcm_set_buffer --------------
  * Sizes in elements; T is the handle's element type.                        */
-#define FFCM_BUF_Y_WRAPPED 0      /* 3N T    particles.Y_wrapped (src/config.jl:75-82)   */
+#define FFCM_BUF_Y_WRAPPED 0      /* 3N T    particles.Y_wrapped (src/config.jl:54-61)   */
 #define FFCM_BUF_Y_SORTED 1       /* 3N T    particles.Y_sorted                          */
 #define FFCM_BUF_F_SORTED 2       /* 3N T    particles.F_sorted                          */
-#define FFCM_BUF_CELL_HASH 3      /* N int32 cells.cell_hash, 0-based (src/config.jl:45-52) */
+#define FFCM_BUF_CELL_HASH 3      /* N int32 cells.cell_hash, 0-based (src/config.jl:24-31) */
 #define FFCM_BUF_ORIGINAL_INDEX 4 /* N int32 cells.original_index, 1-based               */
 #define FFCM_BUF_CELL_START 5     /* ncell int32, 1-based inclusive                      */
 #define FFCM_BUF_CELL_END 6       /* ncell int32, 1-based inclusive (empty: end=start-1) */
 #define FFCM_BUF_FORCE_DENSITY 7  /* 3*Mx*My*Mz T, grid.force_density, x fastest, SoA    */
 #define FFCM_BUF_FLUID_VELOCITY 8 /* 3*Mx*My*Mz T, grid.fluid_velocity                   */
-#define FFCM_BUF_K_X 9            /* Mx/2+1 T  solver.k_x (src/config.jl:374-377)        */
+#define FFCM_BUF_K_X 9            /* Mx/2+1 T  solver.k_x (src/config.jl:353-356)        */
 #define FFCM_BUF_K_Y 10           /* My T      solver.k_y                                */
 #define FFCM_BUF_K_Z 11           /* Mz T      solver.k_z                                */
 #define FFCM_BUF_NEIGHBOR_MAP 12  /* 13*ncell int32, half-shell map, 0-based, get only
@@ -100,15 +100,15 @@ const char* ffcm_last_error(void);
 int ffcm_version(void);
 
 /* Parameter validation of the cold path, no device work.
- * Replaces _validate_config_parameters + the anisotropy check of
- * _derive_scalars (src/config.jl:288-333, 362-369). */
+ * Replaces _validate_config_parameters (src/config.jl:267-312) and the
+ * anisotropy check inside _derive_scalars (lines 341-348 of the same file). */
 int ffcm_validate_config(int32_t dtype, const double* L, double R_c, int64_t N, double a,
                          double kernel_widths_ratio, const int32_t* num_grid_points,
                          int32_t M_G, double viscosity, int32_t fft_planning,
                          int32_t fft_threads);
 
 /* Derived scalars in the working precision (returned widened to double,
- * exactly). Replaces _derive_scalars (src/config.jl:347-380); lets the Julia
+ * exactly). Replaces _derive_scalars (src/config.jl:326-359); lets the Julia
  * side cache them in its FFCMConfig fields. Any output pointer may be NULL. */
 int ffcm_derive_scalars(int32_t dtype, const double* L, double R_c, double a,
                         double kernel_widths_ratio, const int32_t* num_grid_points,
@@ -118,7 +118,7 @@ int ffcm_derive_scalars(int32_t dtype, const double* L, double R_c, double a,
 
 /* Build a configuration on `device`: validates, derives scalars, allocates
  * every hot-path buffer and the FFT tables. Replaces the GPU arm of
- * FFCMConfig{T}(...) (src/config.jl:487-558; ext/ForceCouplingMethodCUDAExt/
+ * FFCMConfig{T}(...) (src/config.jl:466-546; ext/ForceCouplingMethodCUDAExt/
  * config.jl:19-103). */
 int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, int64_t N,
                 double a, double kernel_widths_ratio, const int32_t* num_grid_points,
@@ -128,12 +128,32 @@ int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, i
 /* Release a configuration (finalizer of FFCMConfig). */
 int ffcm_destroy(ffcm_handle* h);
 
+/* ---- stencil offset arithmetic --------------------------------------------
+ * FFCM_OFFSETS_REFERENCE (the default): every Gaussian weight uses the
+ * reference's offset x = T(g) * h - Y with two roundings in T
+ * (src/stencil.jl:105), so Float32 results match the reference's Float32 CPU
+ * backend to round-off. At large boxes that offset cancels two numbers near L
+ * and the Float32 answer itself drifts from the Float64 one (2.2e-4 relative
+ * at L = 275.6, N = 500k).
+ * FFCM_OFFSETS_COMPENSATED: x = fma(g, h, -Y) + g * h_lo, h_lo the rounding
+ * error of h against L / M, so x is rounded once at its own size; Float32
+ * results then follow the Float64 answer to ~1e-5 at that size, and no
+ * longer match the reference's Float32 arithmetic bit for bit (the cell list
+ * and the permutation are unchanged). No reference counterpart.
+ * The mode applies to every later call on the handle (the environment
+ * variable FFCM_STENCIL_OFFSETS=compensated sets it at ffcm_create); changing
+ * it waits for the handle's stream and drops a pending adjoint checkpoint. */
+#define FFCM_OFFSETS_REFERENCE 0
+#define FFCM_OFFSETS_COMPENSATED 1
+int ffcm_set_stencil_offsets(ffcm_handle* h, int32_t mode);
+int ffcm_get_stencil_offsets(const ffcm_handle* h, int32_t* mode);
+
 /* Particle count, element type and cell count of a handle. */
 int ffcm_get_info(const ffcm_handle* h, int64_t* N, int32_t* dtype, int64_t* num_cells_total);
 
 /* ---- launch-shape wisdom --------------------------------------------------
  * The analogue of FFTW wisdom for the reference's `fft_planning = :measure`
- * (src/config.jl:418-423; its cost is the cold path of FFCMConfig): at
+ * (src/config.jl:416-423; its cost is the cold path of FFCMConfig): at
  * ffcm_create the library times the variants of its y and z passes and keeps
  * the fastest per (device, precision, grid); later configurations of the same
  * shape in the process reuse it. These entry points carry the choices across
@@ -149,13 +169,17 @@ int ffcm_get_info(const ffcm_handle* h, int64_t* N, int32_t* dtype, int64_t* num
  * same key); nothing is imported from text with a malformed line
  * (FFCM_ERR_ARGUMENT). A configuration uses an imported choice only if it
  * names variants that configuration can run; otherwise it times them itself.
- * The key holds the device ordinal: wisdom is for the machine that made it. */
+ * The key holds the device ordinal and its SM count: wisdom is for the
+ * machine that made it, and a line made on another GPU model is not used.
+ * Text format: one line per choice, "ffcm-wisdom-2" followed by 13 integers
+ * (ordinal, element size, Mx, My, Mz, SM count, then the 7 fields of
+ * ffcm_get_tuning). */
 int ffcm_get_tuning(const ffcm_handle* h, int32_t* out);
 int64_t ffcm_wisdom_export(char* buf, int64_t cap);
 int ffcm_wisdom_import(const char* text);
 
 /* The assembled operator V = M^VF(Y) F. Replaces mobility!(V, config, Y, F)
- * (src/mobility.jl:309-331) including its staging seam
+ * (src/mobility.jl:23-45) including its staging seam
  * (ext/ForceCouplingMethodCUDAExt/mobility.jl:10-23). Shapes are Julia's
  * (rows, cols) of V, Y, F; anything but (3, N) is FFCM_ERR_DIMENSION. Y and F
  * are never written; V is overwritten in the caller's original order. */
@@ -182,11 +206,11 @@ int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, v
 int ffcm_spread_forces(ffcm_handle* h, void* stream);
 
 /* fluid_velocity = L^-1 force_density. Replaces stokes_solve!
- * (src/stokes_solve.jl:151-240). */
+ * (src/stokes_solve.jl:21-110). */
 int ffcm_stokes_solve(ffcm_handle* h, void* stream);
 
 /* V[:, original_index[s]] = h^3 * gather. Replaces interpolate_velocities!
- * (src/interpolate.jl:263-376). V is 3xN. */
+ * (src/interpolate.jl:23-136). V is 3xN. */
 int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream);
 
 /* V += self and pair correction. Replaces correct_velocities!
@@ -194,7 +218,7 @@ int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* s
 int ffcm_correct_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream);
 
 /* ---- fixed-position operator ----------------------------------------------
- * FFCMMobility(config, Y) applied many times (src/mobility.jl:374-448): the
+ * FFCMMobility(config, Y) applied many times (src/mobility.jl:88-155): the
  * positions are wrapped, hashed and sorted once; every apply re-gathers the
  * forces into that order and solves. The results equal ffcm_mobility's. */
 
@@ -247,7 +271,7 @@ int ffcm_synchronize(ffcm_handle* h, void* stream);
  * built on the first call. No reference counterpart: the reference solves
  * one system and one right-hand side per mobility! call; a batch is
  * equivalent to calling mobility!(V[i][r], config[i], Y[i], F[i][r]) for every
- * system i and right-hand side r (src/mobility.jl:309-331).
+ * system i and right-hand side r (src/mobility.jl:23-45).
  *
  * Shared by all systems: dtype, a, kernel_widths_ratio, M_G, viscosity.
  * Per system i: L[3i..3i+2], R_c[i], N[i], num_grid_points[3i..3i+2].
@@ -274,7 +298,7 @@ int ffcm_batch_get_info(const ffcm_batch* b, int64_t* total_particles, int64_t* 
 /* ---- adjoint form ---------------------------------------------------------
  * Reverse-mode derivative of V = M(Y) F. No reference counterpart: the
  * reference has no derivative; these are the two halves of a
- * ChainRulesCore.rrule for mobility (src/mobility.jl:309-331), the forward
+ * ChainRulesCore.rrule for mobility (src/mobility.jl:23-45), the forward
  * half keeping only the velocity grid u = L^-1 S F (plus the cell list and
  * sorted particles it already holds) and the pullback recomputing stencil
  * weights. All arrays are 3xN in the handle's type. */

@@ -8,7 +8,7 @@ and drives the six steps of `src/mobility.jl`.
 
 Third-party arithmetic the reference delegates:
   * FFTW 3 through FFTW.jl 1.10 (`plan_rfft` / `plan_brfft`,
-    src/config.jl:439-444, src/stokes_solve.jl:151-172). Restated here with
+    src/config.jl:416-423, src/stokes_solve.jl:21-42). Restated here with
     pocketfft (scipy.fft), which computes the same unnormalised forward
     real-to-complex DFT and the same unnormalised backward complex-to-real
     DFT (the imaginary parts of the x-axis DC and Nyquist bins are ignored by
@@ -38,11 +38,11 @@ _lib = None
 
 
 class ArgumentError(ValueError):
-    """Mirror of Julia's ArgumentError raised by FFCMConfig (src/config.jl:288-333)."""
+    """Mirror of Julia's ArgumentError raised by the parameter checks (src/config.jl:267-312)."""
 
 
 class DimensionMismatch(ValueError):
-    """Mirror of Julia's DimensionMismatch raised by mobility! (src/mobility.jl:315-320)."""
+    """Mirror of Julia's DimensionMismatch raised by the shape guard (src/mobility.jl:29-34)."""
 
 
 def build():
@@ -76,7 +76,7 @@ def _ct(T):
 # ----------------------------------------------------------------------------
 
 def _wrap_wavevectors(M, L, T):
-    """src/config.jl:254-258  per-axis wavevectors in FFTW wrap-around order."""
+    """src/config.jl:233-237  per-axis wavevectors in FFTW wrap-around order."""
     twopi = T(2) * T(math.pi)
     half1 = M // 2 + 1
     out = np.empty(M, dtype=T)
@@ -88,7 +88,7 @@ def _wrap_wavevectors(M, L, T):
 
 def validate_config_parameters(T, *, L, R_c, N, a, kernel_widths_ratio, num_grid_points, M_G,
                                viscosity, fft_planning, fft_threads):
-    """src/config.jl:288-333  _validate_config_parameters (first violation raises)."""
+    """src/config.jl:267-312  _validate_config_parameters (first violation raises)."""
     if not R_c > 0:
         raise ArgumentError("R_c must be positive")
     if not all(x > 0 for x in L):
@@ -116,7 +116,7 @@ def validate_config_parameters(T, *, L, R_c, N, a, kernel_widths_ratio, num_grid
 
 
 def derive_scalars(T, *, L, R_c, a, kernel_widths_ratio, num_grid_points):
-    """src/config.jl:347-380  _derive_scalars, in the working precision T."""
+    """src/config.jl:326-359  _derive_scalars, in the working precision T."""
     num_cells = tuple(max(int(np.floor(L[i] / R_c)), 3) for i in range(3))
     cell_size = tuple(L[i] / T(num_cells[i]) for i in range(3))
     inv_cell_size = tuple(T(1) / cell_size[i] for i in range(3))
@@ -141,7 +141,7 @@ def derive_scalars(T, *, L, R_c, a, kernel_widths_ratio, num_grid_points):
 
 
 class OracleConfig:
-    """CPU restatement of `FFCMConfig{T}` (src/config.jl:217-236, 487-558).
+    """CPU restatement of `FFCMConfig{T}` (src/config.jl:196-215, 466-546).
 
     Holds the derived scalars and the hot-path buffers in the reference layouts.
     """
@@ -270,7 +270,7 @@ def build_neighbor_map(num_cells):
 
 
 def modified_kernel_coefficients(sigma, Sigma):
-    """src/stencil.jl:311-320 -> (a0, a2, inv_norm, inv_2Sigma^2)."""
+    """src/stencil.jl:22-31 -> (a0, a2, inv_norm, inv_2Sigma^2)."""
     T = np.asarray(sigma).dtype.type
     out = np.zeros(4, T)
     ct = _ct(T)
@@ -305,7 +305,7 @@ def inverse_transform(cfg, fh):
 
 
 def apply_inverse_stokes_kernel(fh, k_x, k_y, k_z, mu, inv_M):
-    """src/stokes_solve.jl:200-240, in place on fh of shape (3, Mz, My, Mx//2+1)."""
+    """src/stokes_solve.jl:70-110, in place on fh of shape (3, Mz, My, Mx//2+1)."""
     T = np.asarray(k_x).dtype.type
     assert fh.flags.c_contiguous and fh.dtype == np.dtype(np.complex64 if T == np.float32 else np.complex128)
     ct = _ct(T)
@@ -316,7 +316,7 @@ def apply_inverse_stokes_kernel(fh, k_x, k_y, k_z, mu, inv_M):
 
 
 def stokes_solve(cfg):
-    """src/stokes_solve.jl:151-172: force_density -> fluid_velocity."""
+    """src/stokes_solve.jl:21-42: force_density -> fluid_velocity."""
     T = cfg.T
     fh = np.ascontiguousarray(forward_transform(cfg, cfg.force_density))
     Mx, My, Mz = cfg.num_grid_points
@@ -327,7 +327,7 @@ def stokes_solve(cfg):
 
 
 def interpolate_velocities(V, cfg):
-    """src/interpolate.jl:263-282 / 322-376: V[:, original_index[s]] = h^3 * v."""
+    """src/interpolate.jl:23-42 / 322-376: V[:, original_index[s]] = h^3 * v."""
     T = cfg.T
     ct = _ct(T)
     getattr(lib(), "oracle_interpolate" + _sfx(T))(
@@ -368,7 +368,7 @@ def correct_velocities(V, cfg):
 
 
 def mobility(V, cfg, Y, F):
-    """src/mobility.jl:309-331  mobility!(V, config, Y, F) -> V (Y, F untouched)."""
+    """src/mobility.jl:23-45  mobility!(V, config, Y, F) -> V (Y, F untouched)."""
     T = cfg.T
     for name, X in (("V", V), ("Y", Y), ("F", F)):
         X = np.asarray(X)

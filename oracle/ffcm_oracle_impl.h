@@ -134,7 +134,7 @@ void FN(oracle_spread)(FT* f, const FT* Y_sorted, const FT* F_sorted, int64_t N,
     free(g); free(r2); free(idx);
 }
 
-/* src/interpolate.jl:322-376  _interpolate_velocities_kernel!
+/* src/interpolate.jl:82-136  _interpolate_velocities_kernel!
  * Writes V[:, original_index[s]] = h^3 * v (overwrite). */
 void FN(oracle_interpolate)(FT* V, const FT* u, const FT* Y_sorted, const int32_t* original_index,
                            int64_t N, FT sigma, FT Sigma, FT h, FT inv_h, const int32_t* M,
@@ -177,7 +177,7 @@ void FN(oracle_interpolate)(FT* V, const FT* u, const FT* Y_sorted, const int32_
     free(g); free(r2); free(idx);
 }
 
-/* src/stokes_solve.jl:200-240  _apply_inverse_stokes_kernel!
+/* src/stokes_solve.jl:70-110  _apply_inverse_stokes_kernel!
  * fh: three half-complex arrays of shape (nkx, nky, nkz), interleaved (re, im). */
 void FN(oracle_apply_inverse_stokes)(FT* fh, const FT* kx, const FT* ky, const FT* kz,
                                     int64_t nkx, int64_t nky, int64_t nkz, FT mu, FT inv_M) {

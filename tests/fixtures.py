@@ -177,3 +177,29 @@ def clustered_gaussian(N, L, nclusters, seed, log_mean=float(np.log(3.0)), log_s
 def box_for_volume_fraction(N, phi, a=1.0):
     """Cubic box side giving volume fraction phi for N spheres of radius a."""
     return float((N * 4.0 / 3.0 * np.pi * a ** 3 / phi) ** (1.0 / 3.0))
+
+
+def batched_systems(nsys=64, Nmin=2000, Nmax=64000, phi=0.1, h0=0.54, Mmin=64, Mmax=256, R_c=3.0,
+                    seed=2026):
+    """The batched workload's suspensions: N log-uniform in [Nmin, Nmax], a
+    cubic box at volume fraction phi, and the grid the power of two nearest
+    (in log) to L / h0, clamped to [Mmin, Mmax] (so the spacing stays near h0
+    and the grids are 64^3, 128^3 or 256^3)."""
+    rng = np.random.default_rng(seed)
+    Ns = np.exp(rng.uniform(np.log(Nmin), np.log(Nmax), nsys)).astype(np.int64)
+    out = []
+    for n in Ns:
+        L = box_for_volume_fraction(int(n), phi)
+        M = int(2 ** int(np.round(np.log2(L / h0))))
+        M = min(Mmax, max(Mmin, M))
+        out.append(dict(L=(L, L, L), R_c=R_c, N=int(n), num_grid_points=(M, M, M)))
+    return out
+
+
+def batched_inputs(systems, nrhs, seed):
+    """Positions (non-overlapping, uniform) and nrhs N(0, 1) force sets per
+    system, float64: ([Y_i], [[F_i^r]])."""
+    rng = np.random.default_rng(seed + 1)
+    Ys = [nonoverlapping_uniform(s["N"], s["L"][0], seed + 10 + i) for i, s in enumerate(systems)]
+    Fs = [[rng.standard_normal((s["N"], 3)) for _ in range(nrhs)] for s in systems]
+    return Ys, Fs

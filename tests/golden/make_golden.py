@@ -26,8 +26,8 @@ CASES = {
     # test/cuda/test_gpu_mobility.jl random cloud: L=8, 16^3, M_G=8, R_c=1, ratio 2
     "standard_random256": dict(L=8.0, N=256, M=16, M_G=8, R_c=1.0, ratio=2.0, seed=0xC7A0,
                                kind="random"),
-    # L=40, N=2000 non-overlapping, 64^3, M_G=8, R_c=3, ratio 2, N(0,1) forces
-    "c1_N2000_64": dict(L=40.0, N=2000, M=64, M_G=8, R_c=3.0, ratio=2.0, seed=2024 + 0,
+    # the 64^3 workload: L=40, N=2000 non-overlapping, M_G=8, R_c=3, ratio 2, N(0,1) forces
+    "uniform_N2000_64": dict(L=40.0, N=2000, M=64, M_G=8, R_c=3.0, ratio=2.0, seed=2024 + 0,
                         kind="nonoverlap"),
 }
 

@@ -2,9 +2,9 @@
 
 * libffcm_b200.so loads and exports every function include/ffcm_b200.h declares;
 * ffcm_validate_config raises exactly where the reference's constructor does
-  (src/config.jl:288-333, 362-369), compared with the oracle's restatement;
+  (src/config.jl:267-312, 341-348), compared with the oracle's restatement;
 * ffcm_derive_scalars returns the oracle's derived scalars bit for bit, in
-  Float32 and Float64 (src/config.jl:347-380).
+  Float32 and Float64 (src/config.jl:326-359).
 """
 import itertools
 

@@ -1,7 +1,7 @@
 """The oracle's adjoint of the mobility product, pinned two independent ways:
 
 * central finite differences (step 1e-4, Float64) of the oracle's own forward
-  (`mobility`, the restatement of src/mobility.jl:309-331);
+  (`mobility`, the restatement of src/mobility.jl:23-45);
 * reverse-mode automatic differentiation (torch.autograd, Float64) of a
   second, vectorised restatement of the same forward path at N = 2000 (the
   reference's CPU-runnable case: L = 40, 64^3 grid). The reference ships no
@@ -10,7 +10,7 @@
 
 Finite-difference coordinates avoid the two places where the forward is
 discontinuous: the nearest-anchor jump at half-grid positions
-(src/stencil.jl:84, round(Y/h)) and the hard pair cutoff r = R_c
+(src/stencil.jl:97, round(Y/h)) and the hard pair cutoff r = R_c
 (src/correct_velocities.jl:259).
 """
 import math
@@ -104,7 +104,7 @@ def test_adjoint_force_part_is_mobility_of_cotangent(oracle):
 def _torch_objective(cfg, Y, F, Vt):
     """J = 0.5 |V - Vt|^2 with V the mobility product, written with torch ops
     (stencil of src/stencil.jl:80-112, spread src/spread_forces.jl:73-130,
-    Stokes src/stokes_solve.jl:151-240, interpolation src/interpolate.jl:322-376,
+    Stokes src/stokes_solve.jl:21-110, interpolation src/interpolate.jl:82-136,
     correction src/correct_velocities.jl:21-286)."""
     T = torch.float64
     L = float(cfg.L[0])

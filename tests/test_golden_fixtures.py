@@ -10,7 +10,7 @@ import ffcm_oracle as O
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
 
-@pytest.mark.parametrize("name", ["standard_random256", "c1_N2000_64"])
+@pytest.mark.parametrize("name", ["standard_random256", "uniform_N2000_64"])
 @pytest.mark.parametrize("tag,T", [("f32", np.float32), ("f64", np.float64)])
 def test_oracle_reproduces_fixture(name, tag, T):
     z = np.load(GOLDEN / f"{name}.npz")
@@ -27,6 +27,6 @@ def test_oracle_reproduces_fixture(name, tag, T):
 
 
 def test_fixture_f32_close_to_f64():
-    z = np.load(GOLDEN / "c1_N2000_64.npz")
+    z = np.load(GOLDEN / "uniform_N2000_64.npz")
     v32, v64 = z["f32_V"].astype(np.float64), z["f64_V"]
     assert np.linalg.norm(v32 - v64) / np.linalg.norm(v64) < 1e-5

@@ -77,3 +77,52 @@ def test_batch_rejects_bad_shapes(ffcm):
     Y = np.zeros((2000, 3), np.float32)
     with pytest.raises(ffcm.DimensionMismatch):
         batch.mobility(np.zeros((2000, 3), np.float32), Y, np.zeros((2000, 3), np.float32))
+
+
+def test_batched_workload_at_full_size(ffcm):
+    """The batched workload as benchmarked: 64 suspensions (N log-uniform in
+    [2000, 64000], 10% volume fraction, 64^3 / 128^3 / 256^3 grids) with 16
+    right-hand sides each, Float32. Every (system, right-hand side) equals the
+    plain solve of that system; a stratified sample (the smallest and largest
+    system of each grid size, alternating right-hand sides) equals the
+    oracle."""
+    import torch
+    from fixtures import batched_inputs, batched_systems
+    systems = batched_systems(seed=2024 + 2)
+    nrhs = 16
+    Ys, Fs = batched_inputs(systems, nrhs, 2024 + 2)
+    Ys = [y.astype(np.float32) for y in Ys]
+    Fs = [[f.astype(np.float32) for f in fr] for fr in Fs]
+    batch = ffcm.FFCMBatch(np.float32, systems=systems, kernel_widths_ratio=2.0, M_G=8, viscosity=1.0,
+                           nrhs=nrhs)
+    Yf, Ff = batch.pack(Ys, Fs)
+    V = np.empty_like(Ff)
+    batch.mobility(V, Yf, Ff)
+    parts = batch.unpack(V)
+    worst = 0.0
+    for i, s in enumerate(systems):
+        cfg = ffcm.FFCMConfig(np.float32, L=s["L"], R_c=s["R_c"], N=s["N"], kernel_widths_ratio=2.0,
+                              viscosity=1.0, num_grid_points=s["num_grid_points"], M_G=8)
+        Yd = torch.from_numpy(Ys[i]).cuda()
+        for r in range(nrhs):
+            Vp = torch.empty_like(Yd)
+            ffcm.mobility(Vp, cfg, Yd, torch.from_numpy(Fs[i][r]).cuda())
+            torch.cuda.synchronize()
+            e = rel_l2(parts[i][r], Vp.cpu().numpy())
+            worst = max(worst, e)
+        cfg.close()
+    assert worst < 1e-6, worst
+    sample = []
+    for M in sorted({s["num_grid_points"][0] for s in systems}):
+        idx = [i for i, s in enumerate(systems) if s["num_grid_points"][0] == M]
+        idx.sort(key=lambda i: systems[i]["N"])
+        sample += sorted({idx[0], idx[-1]})
+    for k, i in enumerate(sample):
+        s = systems[i]
+        r = (5 * k) % nrhs
+        ora = O.OracleConfig(np.float32, L=s["L"], R_c=s["R_c"], N=s["N"], kernel_widths_ratio=2.0,
+                             viscosity=1.0, num_grid_points=s["num_grid_points"], M_G=8)
+        ora.fft_threads = 8
+        e = rel_l2(parts[i][r], O.apply(ora, Ys[i], Fs[i][r]))
+        assert e < 1e-5, (i, r, e)
+    batch.close()
