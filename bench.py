@@ -85,11 +85,12 @@ def make_inputs():
     return Y, F
 
 
-def algorithmic_bytes(T_bytes=4):
+def algorithmic_bytes(T_bytes=4, geometry=None):
     """Compulsory HBM traffic per solve and per stage (each input read once,
-    each output written once)."""
+    each output written once). geometry = (L, N, M) of another workload (the
+    plain 512^3 one by default)."""
     w = WORK
-    L, N, M3 = work_geometry()
+    L, N, M3 = work_geometry() if geometry is None else geometry
     grid = 3 * int(np.prod(M3)) * T_bytes
     spec = 3 * (M3[0] // 2 + 1) * M3[1] * M3[2] * 2 * T_bytes
     ncell = int(np.prod([max(int(np.floor(np.float32(x) / np.float32(w["R_c"]))), 3) for x in L]))
@@ -199,15 +200,26 @@ def cpu_baseline_run(Y, F, threads, keep=None):
     return sec
 
 
-def accuracy_report(V, Y, F, V32, threads):
+def accuracy_report(V, Y, F, V32, threads, V_comp=None):
     """Errors of the GPU velocities against the oracle: rel-L2 and max-abs
-    against the Float64 restatement, rel-L2 against the Float32 one."""
+    against the Float64 restatement, rel-L2 against the Float32 one; with
+    V_comp, the same for the solve with compensated stencil offsets."""
     import ffcm_oracle as O
     cfg = O.OracleConfig(np.float64, **config_kwargs(), fft_threads=threads)
     V64 = O.apply(cfg, Y.astype(np.float64), F.astype(np.float64))
     V = np.asarray(V, np.float64)
     d64 = V - V64
-    return {"rel_l2_vs_oracle_f64": float(np.linalg.norm(d64) / np.linalg.norm(V64)),
+    comp = None
+    if V_comp is not None:
+        dc = np.asarray(V_comp, np.float64) - V64
+        comp = {"rel_l2_vs_oracle_f64": float(np.linalg.norm(dc) / np.linalg.norm(V64)),
+                "max_abs_vs_oracle_f64": float(np.abs(dc).max()),
+                "rel_l2_vs_oracle_f32": float(np.linalg.norm(np.asarray(V_comp, np.float64) - V32)
+                                              / np.linalg.norm(V32)),
+                "how": "ffcm_set_stencil_offsets(FFCM_OFFSETS_COMPENSATED): stencil offsets "
+                       "fma(g, h, -Y) + g h_lo; same cell list, no longer the reference's Float32 arithmetic"}
+    return {"stencil_offsets_compensated": comp,
+            "rel_l2_vs_oracle_f64": float(np.linalg.norm(d64) / np.linalg.norm(V64)),
             "max_abs_vs_oracle_f64": float(np.abs(d64).max()),
             "max_abs_oracle_f64": float(np.abs(V64).max()),
             "rel_l2_vs_oracle_f32": float(np.linalg.norm(V - V32) / np.linalg.norm(V32)),
@@ -304,6 +316,33 @@ def run_reference(args, rank, world):
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def secondary_workloads(args, local_rank):
+    """Batched, adjoint and clustered measurements for the single-GPU line."""
+    import copy
+    out = {}
+    keep = {
+        "batched": ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config", "plain_looped",
+                    "speedup_vs_plain_looped", "e2e", "roofline", "clocks", "gpu_launches", "result_checksum"),
+        "adjoint": ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config", "forward_ms",
+                    "checkpointed_forward_ms", "pullback_ms", "pullback_cost_vs_forward",
+                    "gradient_step_cost_vs_forward", "e2e", "roofline", "pullback_stage_ms", "clocks",
+                    "gpu_launches"),
+        "clustered": ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config",
+                      "fixed_position_operator_ms_per_rhs", "gradient_ms_per_rhs", "stage_ms", "e2e",
+                      "roofline", "clocks", "gpu_launches"),
+    }
+    runs = (("batched", measure_batched, 10), ("adjoint", measure_adjoint, 10), ("clustered", measure_clustered, 3))
+    for name, fn, steps in runs:
+        a = copy.copy(args)
+        a.steps, a.warmup, a.skip_cpu_baseline = steps, 3, True
+        try:
+            line = fn(a, 0, 1, local_rank)
+            out[name] = {k: line[k] for k in keep[name] if k in line}
+        except Exception as e:   # a failing secondary workload must not hide the headline
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -416,7 +455,13 @@ def run_ours(args, rank, world, local_rank):
                              f"FFT on {cpu_threads} threads (fft_threads)",
                    "single_core": {"value": N / sec1, "unit": UNIT, "cores": 1,
                                    "sample": "the same solve with fft_threads = 1, the reference's default"}}
-            accuracy = accuracy_report(Vh.numpy(), Y, F, kept[0], cpu_threads)
+            # the same solve with the compensated stencil offsets, for the
+            # Float64 comparison (not timed)
+            cfg.stencil_offsets = "compensated"
+            Vc = np.empty_like(Y)
+            ffcm.mobility(Vc, cfg, Y, F)
+            cfg.stencil_offsets = "reference"
+            accuracy = accuracy_report(Vh.numpy(), Y, F, kept[0], cpu_threads, V_comp=Vc)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -439,8 +484,13 @@ def run_ours(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
-        print(json.dumps(line), flush=True)
     cfg.close()
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the secondary workloads on the same box, each with its own CUDA-event
+        # time, clocks and roofline, at reduced step counts
+        line.update(secondary_workloads(args, local_rank))
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -474,6 +524,29 @@ def shard_systems(systems, world):
         owner[i] = r
         load[r] += cost[i]
     return owner
+
+
+def stage_roofline(stage_ms, geometry):
+    """Roofline of the slowest stage of a solve of the given geometry."""
+    per, _ = algorithmic_bytes(geometry=geometry)
+    peak, peak_kind = measured_peak_hbm()
+    ks = [k for k in per if k in stage_ms]
+    if not ks:
+        return None
+    dom = max(ks, key=lambda k: stage_ms[k])
+    ach = per[dom] / (stage_ms[dom] / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
+            "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": per[dom]}
+
+
+def batched_roofline(systems, nrhs, ms):
+    """Whole-batch algorithmic bytes (every system's solve per right-hand side)
+    over the batch time, against the measured HBM peak."""
+    peak, peak_kind = measured_peak_hbm()
+    total = sum(nrhs * algorithmic_bytes(geometry=(s["L"], s["N"], s["num_grid_points"]))[1] for s in systems)
+    ach = total / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": "whole batch", "achieved": ach, "peak": peak, "unit": "GB/s",
+            "frac": ach / peak, "peak_source": peak_kind, "traffic": None, "algorithmic_bytes_per_launch": total}
 
 
 def gather_system_results(mine, parts, nsys, dist, rank):
@@ -511,7 +584,7 @@ def batched_checksum(results):
     return float(sum(np.asarray(v, np.float64).sum() for per_sys in results for v in per_sys))
 
 
-def run_batched(args, rank, world, local_rank):
+def measure_batched(args, rank, world, local_rank):
     import torch
     import importlib.util
     from fixtures import nonoverlapping_uniform
@@ -599,6 +672,7 @@ def run_batched(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     per_sys = [[np.asarray(v, np.float64).sum(axis=0) for v in rhs] for rhs in batch.unpack(Vh.numpy())]
     allres = gather_system_results(mine, per_sys, len(systems_all), dist, rank)
+    line = None
     if rank == 0:
         solves = b["nsys"] * b["nrhs"]
         grids = sorted(set(s["num_grid_points"][0] for s in systems_all))
@@ -617,6 +691,7 @@ def run_batched(args, rank, world, local_rank):
                              "how": "ffcm_mobility per (system, right-hand side), device arrays, "
                                     "one stream"},
             "speedup_vs_plain_looped": ms_plain / ms_batch,
+            "roofline": batched_roofline(systems_all, b["nrhs"], ms_batch * world),
             "e2e": {"value": solves / (ms_e2e / 1e3), "unit": "solves/s", "ms_per_step": ms_e2e,
                     "h2d_bytes_per_step": int(Yh.numel() * 4 + Fh.numel() * 4),
                     "d2h_bytes_per_step": int(Vh.numel() * 4)},
@@ -624,14 +699,13 @@ def run_batched(args, rank, world, local_rank):
             "gpu_launches": int(batch.kernels_per_call * args.steps),
             "result_checksum": batched_checksum(allres),
         }
-        print(json.dumps(line), flush=True)
     batch.close()
     for c in cfgs:
         c.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
+    return line if rank == 0 else None
 
 
 ADJ = dict(L=161.0, N=100_000, M=256, M_G=8, R_c=3.0, ratio=2.0, mu=1.0, perturb=0.05,
@@ -677,7 +751,7 @@ def adjoint_bytes(T_bytes=4):
             "correct": 3 * 16 * N + 4 * N + 2 * 2 * 12 * N}
 
 
-def run_adjoint(args, rank, world, local_rank):
+def measure_adjoint(args, rank, world, local_rank):
     import torch
     ffcm = _load_product()
     torch.cuda.set_device(local_rank)
@@ -741,6 +815,7 @@ def run_adjoint(args, rank, world, local_rank):
         t = torch.tensor([ms_grad, ms_fwd, ms_pull, ms_ckpt, ms_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_grad, ms_fwd, ms_pull, ms_ckpt, ms_e2e = (float(x) for x in t)
+    line = None
     if rank == 0:
         per = adjoint_bytes()
         peak, peak_kind = measured_peak_hbm()
@@ -775,12 +850,11 @@ def run_adjoint(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
-        print(json.dumps(line), flush=True)
     cfg.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
-    return 0
+    return line if rank == 0 else None
 
 
 CLUS = dict(L=300.0, N=2_000_000, M=1024, M_G=8, R_c=3.0, ratio=2.0, mu=1.0, nclusters=2000, nrhs=8,
@@ -793,7 +867,7 @@ def clustered_kwargs():
                 viscosity=c["mu"], num_grid_points=(c["M"],) * 3, M_G=c["M_G"])
 
 
-def run_clustered(args, rank, world, local_rank):
+def measure_clustered(args, rank, world, local_rank):
     """2,000,000 particles in 2,000 Gaussian clusters (L = 300, 1024^3): a plain
     solve, the fixed-position operator over 8 right-hand sides, and the
     objective gradient per right-hand side."""
@@ -881,6 +955,7 @@ def run_clustered(args, rank, world, local_rank):
         t = torch.tensor([ms_plain, ms_apply, ms_grad, ms_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms_plain, ms_apply, ms_grad, ms_e2e = (float(x) for x in t)
+    line = None
     if rank == 0:
         N = c["N"]
         stage_ms = {k: round(v[0] / max(v[1], 1), 4) for k, v in stages.items() if v[1] > 0}
@@ -896,6 +971,7 @@ def run_clustered(args, rank, world, local_rank):
                        "N": N, "grid": [1024] * 3,
                        "l2": "spectrum 12.9 GB >> 126 MB L2; no flush needed",
                        "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": stage_roofline(stage_ms, ((c["L"],) * 3, N, (c["M"],) * 3)),
             "fixed_position_operator_ms_per_rhs": ms_apply / c["nrhs"],
             "gradient_ms_per_rhs": ms_grad / c["nrhs"],
             "stage_ms": stage_ms,
@@ -905,12 +981,29 @@ def run_clustered(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
-        print(json.dumps(line), flush=True)
     cfg.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return line if rank == 0 else None
+
+
+def _print_line(line):
+    if line is not None:
+        print(json.dumps(line), flush=True)
     return 0
+
+
+def run_batched(args, rank, world, local_rank):
+    return _print_line(measure_batched(args, rank, world, local_rank))
+
+
+def run_adjoint(args, rank, world, local_rank):
+    return _print_line(measure_adjoint(args, rank, world, local_rank))
+
+
+def run_clustered(args, rank, world, local_rank):
+    return _print_line(measure_clustered(args, rank, world, local_rank))
 
 
 RES_METRIC = ("particles/s per CG iteration of the resistance solve M(Y) F = V "
@@ -1052,8 +1145,13 @@ def run_resistance(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
-        print(json.dumps(line), flush=True)
     cfg.close()
+    if rank == 0 and world == 1 and not args.no_extras:
+        # the secondary workloads on the same box, each with its own CUDA-event
+        # time, clocks and roofline, at reduced step counts
+        line.update(secondary_workloads(args, local_rank))
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -1088,6 +1186,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="plain workload only: no batched/adjoint/clustered sub-objects")
     ap.add_argument("--workload", choices=["plain", "batched", "adjoint", "clustered", "resistance"], default="plain")
     ap.add_argument("--grid", default=None,
                     help="Mx,My,Mz: smaller case at the same spacing and density (profiling)")

@@ -5,8 +5,8 @@
 // :159-176). The permutation produced here is bit-identical to the reference's
 // serial stable counting sort: a per-cell histogram and exclusive scan give
 // the cell ranges, an atomic-cursor scatter groups each cell's particles, and
-// a per-cell pass restores ascending original order inside each cell (cells
-// hold a handful of particles, so that pass is a short insertion sort).
+// one thread per slot moves its particle to its rank (by original index)
+// inside the cell, which restores the stable order whatever the occupancy.
 #pragma once
 
 #include "common.cuh"
@@ -155,33 +155,30 @@ __global__ void k_scatter_cells(int n_part, const int32_t* __restrict__ key,
     }
 }
 
-// One thread per cell: sort the cell's particle indices ascending (restoring
-// the stable order), write the permutation and gather positions and forces.
+// Stable order inside each cell without a per-cell serial sort: slot_of holds
+// the cell-grouped particle indices in the arbitrary order of the atomic
+// scatter; the particle at slot i moves to off[c] + (the number of particles of
+// its cell with a smaller index), which is its place in the reference's stable
+// counting sort (src/cell_list.jl:64-93). One thread per slot; the cost is the
+// size of the slot's cell, so crowded cells spread over as many threads as
+// they hold particles (the threads of a cell read the same indices, served as
+// broadcasts). Positions and forces are gathered into vec4 records on the way.
 template <typename T>
-__global__ void k_cell_order_gather(int ncell, const int32_t* __restrict__ off,
-                                    int32_t* __restrict__ perm, const T* __restrict__ Yw,
-                                    const T* __restrict__ F, vec4<T>* __restrict__ Ys,
-                                    vec4<T>* __restrict__ Fs) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
-        int b = off[c], e = off[c + 1];
-        // insertion sort in place (cells hold few particles)
-        for (int i = b + 1; i < e; ++i) {
-            int v = perm[i];
-            int j = i - 1;
-            while (j >= b && perm[j] > v) {
-                perm[j + 1] = perm[j];
-                --j;
-            }
-            perm[j + 1] = v;
-        }
-        for (int s = b; s < e; ++s) {
-            int64_t n = perm[s];
-            vec4<T> y, f;
-            y.x = Yw[3 * n]; y.y = Yw[3 * n + 1]; y.z = Yw[3 * n + 2]; y.w = T(0);
-            f.x = F[3 * n]; f.y = F[3 * n + 1]; f.z = F[3 * n + 2]; f.w = T(0);
-            Ys[s] = y;
-            Fs[s] = f;
-        }
+__global__ void k_rank_gather(int n_part, const int32_t* __restrict__ key, const int32_t* __restrict__ off,
+                              const int32_t* __restrict__ slot_of, int32_t* __restrict__ perm,
+                              const T* __restrict__ Yw, const T* __restrict__ F, vec4<T>* __restrict__ Ys,
+                              vec4<T>* __restrict__ Fs) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_part; i += gridDim.x * blockDim.x) {
+        const int n = slot_of[i];
+        const int c = key[n];
+        const int b = off[c], e = off[c + 1];
+        int rank = 0;
+        for (int j = b; j < e; ++j) rank += __ldg(slot_of + j) < n ? 1 : 0;
+        const int dst = b + rank;
+        perm[dst] = n;
+        const int64_t n3 = 3 * (int64_t)n;
+        Ys[dst] = vec4<T>{Yw[n3], Yw[n3 + 1], Yw[n3 + 2], T(0)};
+        Fs[dst] = vec4<T>{F[n3], F[n3 + 1], F[n3 + 2], T(0)};
     }
 }
 

@@ -48,8 +48,14 @@ __device__ __forceinline__ void correction_scalars(T r, const CorrConsts<T>& c, 
         (-c.k11 * ir4 - c.k5 * ir2 * (T(1) + c.k12 * ir2) - c.k13) * DS;
 }
 
+// x - L round(x / L), ties to even (src/correct_velocities.jl:121-127). For
+// |x| <= L/2 the correctly rounded quotient is at most 1/2 in magnitude, so
+// the rounded multiple is 0 and the reference's expression returns x (up to
+// the sign of a zero x, which no later sum or comparison sees): the division
+// is only evaluated for separations that may wrap.
 template <typename T>
 __device__ __forceinline__ T min_image(T x, T L) {
+    if (fabs(x) <= T(0.5) * L) return x;
     return sub_rn(x, mul_rn(L, rint_t(div_rn(x, L))));
 }
 

@@ -411,6 +411,7 @@ struct Engine final : EngineBase {
     // slab kernels: spread/interpolation fused with the x transforms
     bool slab = false;
     SlabKernels<T> sk;
+    int spread_kind = 0;   // FFCM_SPREAD: 0 tile owner, 1 pairs
     SlabGeom sg;
     T* partial = nullptr;
     int* slab_lists = nullptr;   // per-slab particle lists kept by the spread
@@ -567,6 +568,16 @@ struct Engine final : EngineBase {
             sg.lcap = (int)std::min<double>(1 << 20, std::max(256.0, 4.0 * expect + 64.0));
             sg.lcap = (sg.lcap + 31) / 32 * 32;
             TRY(raise_smem_cap((const void*)sk.spread_fused, sk.smem));
+            TRY(raise_smem_cap((const void*)sk.spread_pp, sk.smem_pp));
+            {
+                // spread window processing: 0 = per grid point (tile owner,
+                // deterministic), 1 = per (entry, x offset) pair with
+                // shared-memory atomics
+                const char* v = std::getenv("FFCM_SPREAD");
+                if (v && std::strcmp(v, "tile") == 0) spread_kind = 0;
+                else if (v && std::strcmp(v, "pairs") == 0) spread_kind = 1;
+                else if (v && *v) return fail(FFCM_ERR_ARGUMENT, "FFCM_SPREAD must be \"tile\" or \"pairs\"");
+            }
             TRY(raise_smem_cap((const void*)sk.interp, sk.smem_interp));
         }
         if (fast_y) {
@@ -969,9 +980,10 @@ struct Engine final : EngineBase {
                    (const int32_t*)tiles, off));
         CUDA_TRY(cudaMemsetAsync(cnt, 0, (size_t)ncell * sizeof(int32_t), s));
         TRY(launch(h, k_scatter_cells, grid_for(N, 256), 256, 0, s, N, (const int32_t*)key,
-                   (const int32_t*)off, cnt, perm));
-        return launch(h, k_cell_order_gather<T>, grid_for(ncell, 256), 256, 0, s, ncell,
-                      (const int32_t*)off, perm, (const T*)Yw, static_cast<const T*>(F), Ys, Fs);
+                   (const int32_t*)off, cnt, scratch_i));
+        return launch(h, k_rank_gather<T>, grid_for(N, 256), 256, 0, s, N, (const int32_t*)key,
+                      (const int32_t*)off, (const int32_t*)scratch_i, perm, (const T*)Yw,
+                      static_cast<const T*>(F), Ys, Fs);
     }
 
     // Hot path of the assembled operator: spread straight into the x-transformed
@@ -985,7 +997,9 @@ struct Engine final : EngineBase {
             TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
                        slab_lists, slab_counts));
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys, force ? force : (const vec4<T>*)Fs,
+        return launch(h, spread_kind == 1 ? sk.spread_pp : sk.spread_fused, g, 256,
+                      spread_kind == 1 ? sk.smem_pp : sk.smem, s, (const vec4<T>*)Ys,
+                      force ? force : (const vec4<T>*)Fs,
                       (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, (const int*)slab_lists,
                       (const int*)slab_counts);
     }
