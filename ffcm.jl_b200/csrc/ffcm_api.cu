@@ -2509,12 +2509,27 @@ __global__ void k_noalloc_scatter(int n_part, const int32_t* __restrict__ key, i
     }
 }
 
+// Cells of up to this many particles are put in order by one thread each
+// (insertion sort); larger ones are listed for k_noalloc_sort_large.
+constexpr int kNoallocSmallCell = 32;
+// Cells up to this size are sorted by one block in shared memory.
+constexpr int kNoallocBlockCell = 8192;
+
 // Per cell: ascending original order (stability), 1-based indices, and the
 // reference's 1-based inclusive ranges (an empty cell has start = end + 1).
+// Crowded cells are appended to `large` (count in *nlarge) and finished by
+// k_noalloc_sort_large, so no thread sorts more than kNoallocSmallCell values.
 __global__ void k_noalloc_finish(int ncell, const int32_t* __restrict__ off, int32_t* __restrict__ idx,
-                                 int32_t* __restrict__ cell_start, int32_t* __restrict__ cell_end) {
+                                 int32_t* __restrict__ cell_start, int32_t* __restrict__ cell_end,
+                                 int32_t* __restrict__ large, int32_t* __restrict__ nlarge) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < ncell; c += gridDim.x * blockDim.x) {
         const int b = off[c], e = off[c + 1];
+        cell_start[c] = b + 1;
+        cell_end[c] = e;
+        if (e - b > kNoallocSmallCell) {
+            large[atomicAdd(nlarge, 1)] = c;
+            continue;
+        }
         for (int i = b + 1; i < e; ++i) {
             const int v = idx[i];
             int j = i - 1;
@@ -2525,8 +2540,46 @@ __global__ void k_noalloc_finish(int ncell, const int32_t* __restrict__ off, int
             idx[j + 1] = v;
         }
         for (int i = b; i < e; ++i) idx[i] += 1;
-        cell_start[c] = b + 1;
-        cell_end[c] = e;
+    }
+}
+
+// One block per crowded cell (grid-stride over the list): the cell's indices
+// are staged in shared memory, each one's rank (the number of smaller ones,
+// all distinct) is counted there, and the block writes them back in order,
+// 1-based. A cell beyond kNoallocBlockCell is sorted by a single thread in
+// place (a degenerate input: every particle in a handful of cells).
+__global__ void k_noalloc_sort_large(const int32_t* __restrict__ off, int32_t* __restrict__ idx,
+                                     const int32_t* __restrict__ large, const int32_t* __restrict__ nlarge) {
+    __shared__ int32_t vals[kNoallocBlockCell];
+    const int count = *nlarge;
+    for (int q = blockIdx.x; q < count; q += gridDim.x) {
+        const int c = large[q];
+        const int b = off[c], n = off[c + 1] - b;
+        if (n > kNoallocBlockCell) {
+            if (threadIdx.x == 0) {
+                for (int i = b + 1; i < b + n; ++i) {
+                    const int v = idx[i];
+                    int j = i - 1;
+                    while (j >= b && idx[j] > v) {
+                        idx[j + 1] = idx[j];
+                        --j;
+                    }
+                    idx[j + 1] = v;
+                }
+                for (int i = b; i < b + n; ++i) idx[i] += 1;
+            }
+            __syncthreads();
+            continue;
+        }
+        for (int i = threadIdx.x; i < n; i += blockDim.x) vals[i] = idx[b + i];
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += blockDim.x) {
+            const int v = vals[i];
+            int rank = 0;
+            for (int j = 0; j < n; ++j) rank += vals[j] < v ? 1 : 0;
+            idx[b + rank] = v + 1;
+        }
+        __syncthreads();   // vals is reused by the next cell
     }
 }
 
@@ -2576,8 +2629,18 @@ extern "C" int ffcm_sort_cells_noalloc(const int32_t* cell_hash, int64_t N, int3
         k_noalloc_scatter<<<grid_for(n, 256), 256, 0, s>>>(n, cell_hash, ncell, off, cnt, original_index);
         TRY(chk("k_noalloc_scatter"));
     }
-    k_noalloc_finish<<<grid_for(ncell, 256), 256, 0, s>>>(ncell, off, original_index, cell_start, cell_end);
+    // the cursors and the scan's tile sums are consumed: the cursor space
+    // holds the list of crowded cells (fewer than ncell) and the first tile
+    // sum its length
+    int32_t* large = cnt;
+    int32_t* nlarge = tiles;
+    k_noalloc_zero<<<1, 32, 0, s>>>(nlarge, 1, nullptr);
+    TRY(chk("k_noalloc_zero"));
+    k_noalloc_finish<<<grid_for(ncell, 256), 256, 0, s>>>(ncell, off, original_index, cell_start, cell_end,
+                                                           large, nlarge);
     TRY(chk("k_noalloc_finish"));
+    k_noalloc_sort_large<<<148 * 2, 256, 0, s>>>(off, original_index, large, nlarge);
+    TRY(chk("k_noalloc_sort_large"));
     int32_t bad = 0;
     CUDA_TRY(cudaMemcpyAsync(&bad, flag, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));

@@ -76,3 +76,29 @@ def test_noalloc_sort_rejects_bad_sizes_and_keys(ffcm):
     counts = np.bincount(k, minlength=ncell)
     np.testing.assert_array_equal(ce.cpu().numpy(), np.cumsum(counts))
     np.testing.assert_array_equal(cs.cpu().numpy(), np.cumsum(counts) - counts + 1)
+
+
+@pytest.mark.parametrize("N,ncell,crowd", [(50_000, 27, None), (12_000, 1000, 10_000), (4000, 5000, 33)])
+def test_noalloc_sort_crowded_cells(ffcm, N, ncell, crowd):
+    """Crowded cells (more than 32 particles) are put in order by a block in
+    shared memory, and a cell beyond 8192 by one thread; the result is the
+    stable order either way, twice in a row."""
+    torch = pytest.importorskip("torch")
+    lib = ffcm._lib.load()
+    sort = _noalloc(lib)
+    rng = np.random.default_rng(N + ncell)
+    k = rng.integers(0, ncell, N).astype(np.int32)
+    if crowd is not None:
+        k[rng.permutation(N)[:crowd]] = 7      # one cell with `crowd` (or more) particles
+    key = torch.from_numpy(k).cuda()
+    outs = [torch.empty(N, dtype=torch.int32, device="cuda"), torch.empty(ncell, dtype=torch.int32, device="cuda"),
+            torch.empty(ncell, dtype=torch.int32, device="cuda")]
+    counts = np.bincount(k, minlength=ncell)
+    for _ in range(2):
+        for o in outs:
+            o.fill_(-7)
+        rc = sort(key.data_ptr(), N, ncell, outs[0].data_ptr(), outs[1].data_ptr(), outs[2].data_ptr(), None)
+        assert rc == 0, ffcm._lib.last_error()
+        np.testing.assert_array_equal(outs[0].cpu().numpy(), np.argsort(k, kind="stable") + 1)
+        np.testing.assert_array_equal(outs[2].cpu().numpy(), np.cumsum(counts))
+        np.testing.assert_array_equal(outs[1].cpu().numpy(), np.cumsum(counts) - counts + 1)
