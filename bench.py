@@ -203,7 +203,7 @@ def cpu_baseline_run(Y, F, threads, keep=None):
 def accuracy_report(V, Y, F, V32, threads, V_comp=None):
     """Errors of the GPU velocities against the oracle: rel-L2 and max-abs
     against the Float64 restatement, rel-L2 against the Float32 one; with
-    V_comp, the same for the solve with compensated stencil offsets."""
+    V_comp, the same for the solve with Float64 stencil geometry."""
     import ffcm_oracle as O
     cfg = O.OracleConfig(np.float64, **config_kwargs(), fft_threads=threads)
     V64 = O.apply(cfg, Y.astype(np.float64), F.astype(np.float64))
@@ -216,9 +216,10 @@ def accuracy_report(V, Y, F, V32, threads, V_comp=None):
                 "max_abs_vs_oracle_f64": float(np.abs(dc).max()),
                 "rel_l2_vs_oracle_f32": float(np.linalg.norm(np.asarray(V_comp, np.float64) - V32)
                                               / np.linalg.norm(V32)),
-                "how": "ffcm_set_stencil_offsets(FFCM_OFFSETS_COMPENSATED): stencil offsets "
-                       "fma(g, h, -Y) + g h_lo; same cell list, no longer the reference's Float32 arithmetic"}
-    return {"stencil_offsets_compensated": comp,
+                "how": "ffcm_set_stencil(FFCM_STENCIL_FLOAT64): stencil anchors and offsets from the "
+                       "double box spacing, weights in Float32; same cell list, not the reference's "
+                       "Float32 arithmetic"}
+    return {"stencil_float64": comp,
             "rel_l2_vs_oracle_f64": float(np.linalg.norm(d64) / np.linalg.norm(V64)),
             "max_abs_vs_oracle_f64": float(np.abs(d64).max()),
             "max_abs_oracle_f64": float(np.abs(V64).max()),
@@ -455,12 +456,12 @@ def run_ours(args, rank, world, local_rank):
                              f"FFT on {cpu_threads} threads (fft_threads)",
                    "single_core": {"value": N / sec1, "unit": UNIT, "cores": 1,
                                    "sample": "the same solve with fft_threads = 1, the reference's default"}}
-            # the same solve with the compensated stencil offsets, for the
-            # Float64 comparison (not timed)
-            cfg.stencil_offsets = "compensated"
+            # the same solve with Float64 stencil geometry, for the Float64
+            # comparison (not timed)
+            cfg.stencil = "float64"
             Vc = np.empty_like(Y)
             ffcm.mobility(Vc, cfg, Y, F)
-            cfg.stencil_offsets = "reference"
+            cfg.stencil = "reference"
             accuracy = accuracy_report(Vh.numpy(), Y, F, kept[0], cpu_threads, V_comp=Vc)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,

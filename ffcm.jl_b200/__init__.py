@@ -163,18 +163,19 @@ class FFCMConfig:
     ``gpu_acceleration`` must be true: this configuration always lives on the
     GPU; the CPU backend is the reference's own.
 
-    ``stencil_offsets`` (no reference counterpart): ``"reference"`` (default)
-    computes every stencil offset ``g h - Y`` with the reference's Float32
-    arithmetic, so results match its CPU backend to round-off;
-    ``"compensated"`` rounds the offset once at its own size
-    (``ffcm_set_stencil_offsets``), which keeps Float32 results near the
-    Float64 answer in large boxes. ``None`` keeps the library's default (the
-    ``FFCM_STENCIL_OFFSETS`` environment variable, else ``"reference"``).
+    ``stencil`` (no reference counterpart): ``"reference"`` (default) picks
+    each stencil's anchor and offsets with the reference's arithmetic in
+    precision T, so results match its CPU backend to round-off; ``"float64"``
+    picks them in double precision from the box length as given
+    (``ffcm_set_stencil``), which keeps Float32 results at the Float64 answer
+    where Float32 anchors would flip (large boxes). ``None`` keeps the
+    library's default (the ``FFCM_STENCIL`` environment variable, else
+    ``"reference"``).
     """
 
     def __init__(self, T=np.float32, *, L, R_c, N, a=1.0, kernel_widths_ratio,
                  num_grid_points, M_G, viscosity, fft_planning="measure", fft_threads=1,
-                 gpu_acceleration=True, device=0, stencil_offsets=None):
+                 gpu_acceleration=True, device=0, stencil=None):
         self._h = None
         self.T = np.dtype(T).type
         dt = _dtype_code(T)
@@ -214,21 +215,21 @@ class FFCMConfig:
         self.sigma, self.Sigma = T_(s.value), T_(S.value)
         self.h, self.inv_h = T_(hh.value), T_(ih.value)
         self.num_cells_total = int(np.prod(self.num_cells))
-        if stencil_offsets is not None:
-            self.stencil_offsets = stencil_offsets
+        if stencil is not None:
+            self.stencil = stencil
 
     @property
-    def stencil_offsets(self):
-        """``"reference"`` or ``"compensated"`` (see the class docstring)."""
+    def stencil(self):
+        """``"reference"`` or ``"float64"`` (see the class docstring)."""
         m = ctypes.c_int32(0)
-        _raise(L_.load().ffcm_get_stencil_offsets(self.handle, ctypes.byref(m)))
-        return {v: k for k, v in L_.OFFSETS.items()}[m.value]
+        _raise(L_.load().ffcm_get_stencil(self.handle, ctypes.byref(m)))
+        return {v: k for k, v in L_.STENCIL.items()}[m.value]
 
-    @stencil_offsets.setter
-    def stencil_offsets(self, mode):
-        if mode not in L_.OFFSETS:
-            raise ArgumentError(f"stencil_offsets must be 'reference' or 'compensated'; got {mode!r}")
-        _raise(L_.load().ffcm_set_stencil_offsets(self.handle, L_.OFFSETS[mode]))
+    @stencil.setter
+    def stencil(self, mode):
+        if mode not in L_.STENCIL:
+            raise ArgumentError(f"stencil must be 'reference' or 'float64'; got {mode!r}")
+        _raise(L_.load().ffcm_set_stencil(self.handle, L_.STENCIL[mode]))
 
     # -- lifetime ---------------------------------------------------------
     def close(self):

@@ -36,8 +36,8 @@ DEVICE = 1
 
 FFT_PLANNING = {"estimate": 0, "measure": 1, "patient": 2}
 
-# stencil offset arithmetic (ffcm_set_stencil_offsets)
-OFFSETS = {"reference": 0, "compensated": 1}
+# stencil arithmetic (ffcm_set_stencil)
+STENCIL = {"reference": 0, "float64": 1}
 
 BUF = dict(Y_WRAPPED=0, Y_SORTED=1, F_SORTED=2, CELL_HASH=3, ORIGINAL_INDEX=4, CELL_START=5,
            CELL_END=6, FORCE_DENSITY=7, FLUID_VELOCITY=8, K_X=9, K_Y=10, K_Z=11,
@@ -65,8 +65,8 @@ SIGNATURES = {
                                _i32, _i32, _i32]),
     "ffcm_destroy": (_c.c_int, [_vp]),
     "ffcm_get_info": (_c.c_int, [_vp, _i64p, _i32p, _i64p]),
-    "ffcm_set_stencil_offsets": (_c.c_int, [_vp, _i32]),
-    "ffcm_get_stencil_offsets": (_c.c_int, [_vp, _i32p]),
+    "ffcm_set_stencil": (_c.c_int, [_vp, _i32]),
+    "ffcm_get_stencil": (_c.c_int, [_vp, _i32p]),
     "ffcm_get_tuning": (_c.c_int, [_vp, _i32p]),
     "ffcm_wisdom_export": (_i64, [_c.c_char_p, _i64]),
     "ffcm_wisdom_import": (_c.c_int, [_c.c_char_p]),

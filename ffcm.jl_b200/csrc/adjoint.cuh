@@ -73,11 +73,11 @@ __global__ void k_adjoint_gather(int n_part, const vec4<T>* __restrict__ Ys, con
             const int axis = e / MG, k = e - axis * MG;
             const T yy = axis == 0 ? y.x : (axis == 1 ? y.y : y.z);
             const int M = axis == 0 ? p.Mx : (axis == 1 ? p.My : p.Mz);
-            const int j = (int)rint_t(mul_rn(yy, p.inv_h));
+            const int j = stencil_anchor(p, yy);
             const int gi = j + (k - p.half);
             // one rounding (fused multiply-add) instead of the forward's two:
             // the gradient sums cancel strongly, so the offset's accuracy
-            // matters more here than in the forward; with compensated offsets
+            // matters more here than in the forward; with Float64 stencil geometry
             // the forward's own (more accurate) offset
             const T x = p.comp ? stencil_offset(p, gi, yy) : fma_t((T)gi, p.h, -yy);
             g[e] = p.inv_norm * exp_t(-x * x * p.inv_2S2);

@@ -267,8 +267,8 @@ struct EngineBase {
     virtual void* adj_buf(int which) = 0;  // 0 lambda, 1 dY, 2 dF, 3 target, 4 J (double)
     virtual int ensure_real_grids() = 0;
     virtual bool uses_slab() const = 0;
-    // stencil offset arithmetic of every later launch (FFCM_OFFSETS_*)
-    virtual void set_offsets(int mode) = 0;
+    // stencil arithmetic of every later launch (FFCM_STENCIL_*)
+    virtual void set_stencil(int mode) = 0;
     // the y/z variant in use: ykind, By, ygrid, zkind, Bz, zgrid, kx_chunk
     // (-1 for an axis without the power-of-two passes)
     virtual void tuning(int32_t* out) const = 0;
@@ -294,7 +294,7 @@ struct ffcm_handle {
     int64_t N = 0;
     int32_t M[3] = {0, 0, 0};
     int32_t M_G = 0;
-    int32_t offsets = FFCM_OFFSETS_REFERENCE;   // stencil offset arithmetic
+    int32_t stencil = FFCM_STENCIL_REFERENCE;   // stencil arithmetic (FFCM_STENCIL_*)
     int32_t num_cells[3] = {0, 0, 0};
     int64_t ncell = 0;
     size_t esize = 4;
@@ -473,9 +473,15 @@ struct Engine final : EngineBase {
         sp.a2 = dd / (T(2) * S4);
         sp.inv_norm = T(1) / std::sqrt(T(2) * T(kPi) * S2);
         sp.inv_2S2 = T(1) / (T(2) * S2);
-        // rounding error of h against the exact spacing of the box in T
-        sp.h_lo = T((long double)L[0] / (long double)Mx - (long double)d.h);
-        sp.comp = h->offsets == FFCM_OFFSETS_COMPENSATED ? 1 : 0;
+        // the box spacing as the caller gave it (double), for Float64-geometry
+        // stencils: as the Float64 reference computes h = L / M, inv_h = 1 / h
+        {
+            const double hd = Ld[0] / (double)Mx;
+            sp.inv_hd = 1.0 / hd;
+            sp.h_hi = T(hd);
+            sp.h_lo = T(hd - (double)sp.h_hi);
+        }
+        sp.comp = h->stencil == FFCM_STENCIL_FLOAT64 ? 1 : 0;
         h3 = d.h * d.h * d.h;
         const T inv_M = T(1) / T((double)plane);
         inv_mu_M = inv_M / mu;
@@ -950,7 +956,7 @@ struct Engine final : EngineBase {
     }
 
     bool uses_slab() const override { return slab; }
-    void set_offsets(int mode) override { sp.comp = mode == FFCM_OFFSETS_COMPENSATED ? 1 : 0; }
+    void set_stencil(int mode) override { sp.comp = mode == FFCM_STENCIL_FLOAT64 ? 1 : 0; }
 
     int gather_forces(const void* F, cudaStream_t s) override {
         StageScope sc(h, FFCM_STAGE_CELL_LIST, s);
@@ -1528,10 +1534,10 @@ int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, i
     h->M_G = M_G;
     h->esize = dtype == FFCM_FLOAT32 ? 4 : 8;
     {
-        const char* v = std::getenv("FFCM_STENCIL_OFFSETS");
-        if (v && std::strcmp(v, "compensated") == 0) h->offsets = FFCM_OFFSETS_COMPENSATED;
+        const char* v = std::getenv("FFCM_STENCIL");
+        if (v && std::strcmp(v, "float64") == 0) h->stencil = FFCM_STENCIL_FLOAT64;
         else if (v && *v && std::strcmp(v, "reference") != 0)
-            return fail(FFCM_ERR_ARGUMENT, "FFCM_STENCIL_OFFSETS must be \"reference\" or \"compensated\"");
+            return fail(FFCM_ERR_ARGUMENT, "FFCM_STENCIL must be \"reference\" or \"float64\"");
     }
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMalloc(&h->d_err, sizeof(int)));
@@ -1625,17 +1631,17 @@ int ffcm_wisdom_import(const char* text) {
     return FFCM_OK;
 }
 
-int ffcm_set_stencil_offsets(ffcm_handle* h, int32_t mode) {
+int ffcm_set_stencil(ffcm_handle* h, int32_t mode) {
     g_err.clear();
     TRY(check_handle(h));
-    if (mode != FFCM_OFFSETS_REFERENCE && mode != FFCM_OFFSETS_COMPENSATED)
-        return fail(FFCM_ERR_ARGUMENT, "mode must be FFCM_OFFSETS_REFERENCE or FFCM_OFFSETS_COMPENSATED");
-    if (mode == h->offsets) return FFCM_OK;
+    if (mode != FFCM_STENCIL_REFERENCE && mode != FFCM_STENCIL_FLOAT64)
+        return fail(FFCM_ERR_ARGUMENT, "mode must be FFCM_STENCIL_REFERENCE or FFCM_STENCIL_FLOAT64");
+    if (mode == h->stencil) return FFCM_OK;
     DeviceGuard g(h->device);
     // work already queued keeps the mode it was launched with
     if (h->stream) CUDA_TRY(cudaStreamSynchronize(h->stream));
-    h->offsets = mode;
-    h->eng->set_offsets(mode);
+    h->stencil = mode;
+    h->eng->set_stencil(mode);
     // a checkpoint was made with the other weights, and the conjugate-gradient
     // graph holds the old kernel parameters: neither may be reused
     h->ckpt = false;
@@ -1643,10 +1649,10 @@ int ffcm_set_stencil_offsets(ffcm_handle* h, int32_t mode) {
     return FFCM_OK;
 }
 
-int ffcm_get_stencil_offsets(const ffcm_handle* h, int32_t* mode) {
+int ffcm_get_stencil(const ffcm_handle* h, int32_t* mode) {
     TRY(check_handle(h));
     if (!mode) return fail(FFCM_ERR_ARGUMENT, "mode must not be NULL");
-    *mode = h->offsets;
+    *mode = h->stencil;
     return FFCM_OK;
 }
 

@@ -144,9 +144,9 @@ template <typename T, int BY, int BZ>
 __device__ __forceinline__ void slab_anchor(const StencilParams<T>& p, const vec4<T>& y, int y0r, int z0r,
                                             int& sx, int& sy, int& sz, unsigned& m) {
     constexpr int half = SLAB_MG / 2;
-    sx = (int)rint_t(mul_rn(y.x, p.inv_h)) - half;
-    sy = (int)rint_t(mul_rn(y.y, p.inv_h)) - half;
-    sz = (int)rint_t(mul_rn(y.z, p.inv_h)) - half;
+    sx = stencil_anchor(p, y.x) - half;
+    sy = stencil_anchor(p, y.y) - half;
+    sz = stencil_anchor(p, y.z) - half;
     const unsigned my = rows_hit<BY>(sy, y0r, p.My);
     const unsigned mz = rows_hit<BZ>(sz, z0r, p.Mz);
     m = (my && mz) ? (my | (mz << 8)) : 0u;
@@ -781,7 +781,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
             ss[u] = 0;
             if (t < stored) {
                 ss[u] = glist[t];
-                const int x0 = wrap1((int)rint_t(mul_rn(Ys[ss[u]].x, p.inv_h)) - SLAB_MG / 2, Mx);
+                const int x0 = wrap1(stencil_anchor(p, Ys[ss[u]].x) - SLAB_MG / 2, Mx);
                 res[u] = x0 & 31;
                 rk[u] = atomicAdd(&s_cnt[res[u]], 1);
             }

@@ -18,26 +18,38 @@ template <typename T>
 struct StencilParams {
     int Mx, My, Mz, MG, half;
     T h, inv_h, a0, a2, inv_norm, inv_2S2;
-    // compensated stencil offsets (opt-in): h_lo is the rounding error of h
-    // against the exact spacing L / M of the configuration's box
-    T h_lo;
+    // Float64-geometry stencils (opt-in, comp = 1): the spacing of the box as
+    // the caller gave it, in double (inv_hd = 1 / (L / M)), and split into two
+    // T values h_hi + h_lo
+    double inv_hd;
+    T h_hi, h_lo;
     int comp;
 };
 
-// Offset x = g h - y of stencil point g from a particle at y.
-//  * reference arithmetic (comp = 0; src/stencil.jl:105, `T.(g) .* h .- Y`):
-//    the product g h is rounded to T before the subtraction. When g h and y
-//    are both near the box length L the difference keeps only the bits the
-//    two roundings leave, an absolute error of order ulp(L) (3e-5 at
-//    L = 275.6 in Float32) in every Gaussian weight;
-//  * compensated (comp = 1): h = h + h_lo as a two-term split of the exact
-//    spacing, x = fma(g, h, -y) + g h_lo, so x is rounded once at its own
-//    size (~M_G h / 2): the Float32 result then sits within the Float64
-//    answer's 1e-5 instead of 2e-4 at that box size. Bit parity with the
-//    reference's Float32 arithmetic is given up, so this is not the default.
+// Which grid points a particle's stencil covers and how far they are from it.
+//  * reference arithmetic (comp = 0; src/stencil.jl:97-105): the anchor
+//    j = round(Y inv_h) and the offsets x = T(g) h - Y in the working precision
+//    T. In Float32 the anchor of a particle whose Y / h lies within a few
+//    ulp(Y / h) of a half-integer can differ from the one Float64 arithmetic
+//    picks (and, at a box length like 275.6 that Float32 cannot represent,
+//    from the one of the box the caller meant); the truncated M_G-point
+//    stencil then covers a neighbouring set of points. Those particles carry
+//    most of the Float32 result's distance from the Float64 one (2.2e-4
+//    relative at N = 500k, L = 275.6, 512^3).
+//  * Float64 geometry (comp = 1): the anchor is rounded from the double product
+//    Y inv_hd, so it is the Float64 reference's choice, and the offset is
+//    fma(g, h_hi, -Y) + g h_lo, rounded once at its own size. The weights
+//    themselves stay in T. Bit parity with the reference's Float32 arithmetic
+//    is given up, so this is not the default.
+template <typename T>
+__device__ __forceinline__ int stencil_anchor(const StencilParams<T>& p, T y) {
+    if (p.comp) return (int)rint(__dmul_rn((double)y, p.inv_hd));
+    return (int)rint_t(mul_rn(y, p.inv_h));
+}
+
 template <typename T>
 __device__ __forceinline__ T stencil_offset(const StencilParams<T>& p, int g, T y) {
-    if (p.comp) return fma_t((T)g, p.h, -y) + (T)g * p.h_lo;
+    if (p.comp) return fma_t((T)g, p.h_hi, -y) + (T)g * p.h_lo;
     return sub_rn(mul_rn((T)g, p.h), y);
 }
 
@@ -58,7 +70,7 @@ __device__ __forceinline__ void fill_stencil_warp(const StencilParams<T>& p, T y
         int axis = e / p.MG, k = e - axis * p.MG;
         T y = axis == 0 ? y0 : (axis == 1 ? y1 : y2);
         int M = axis == 0 ? p.Mx : (axis == 1 ? p.My : p.Mz);
-        int j = (int)rint_t(mul_rn(y, p.inv_h));
+        int j = stencil_anchor(p, y);
         int g = j + (k - p.half);
         T x = stencil_offset(p, g, y);
         T x2 = mul_rn(x, x);

@@ -128,25 +128,29 @@ int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, i
 /* Release a configuration (finalizer of FFCMConfig). */
 int ffcm_destroy(ffcm_handle* h);
 
-/* ---- stencil offset arithmetic --------------------------------------------
- * FFCM_OFFSETS_REFERENCE (the default): every Gaussian weight uses the
- * reference's offset x = T(g) * h - Y with two roundings in T
- * (src/stencil.jl:105), so Float32 results match the reference's Float32 CPU
- * backend to round-off. At large boxes that offset cancels two numbers near L
- * and the Float32 answer itself drifts from the Float64 one (2.2e-4 relative
- * at L = 275.6, N = 500k).
- * FFCM_OFFSETS_COMPENSATED: x = fma(g, h, -Y) + g * h_lo, h_lo the rounding
- * error of h against L / M, so x is rounded once at its own size; Float32
- * results then follow the Float64 answer to ~1e-5 at that size, and no
- * longer match the reference's Float32 arithmetic bit for bit (the cell list
- * and the permutation are unchanged). No reference counterpart.
+/* ---- stencil arithmetic ----------------------------------------------------
+ * FFCM_STENCIL_REFERENCE (the default): the stencil anchor j = round(Y inv_h)
+ * and the offsets x = T(g) * h - Y are computed in the working precision T, as
+ * the reference does (src/stencil.jl:97-105), so Float32 results match the
+ * reference's Float32 CPU backend to round-off. Where Y / h lies within a few
+ * Float32 ulps of a half-integer, that anchor can differ from the one Float64
+ * arithmetic picks (and from the one of the box the caller meant, when L is
+ * not representable in Float32), and the truncated M_G-point stencil then
+ * covers neighbouring points: at N = 500k, L = 275.6, 512^3 those few dozen
+ * particles put the Float32 answer 2.2e-4 (relative L2) from the Float64 one.
+ * FFCM_STENCIL_FLOAT64: anchors rounded from the double product Y * (M / L),
+ * with L as passed to ffcm_create, and offsets fma(g, h_hi, -Y) + g * h_lo
+ * with h_hi + h_lo the double spacing; the weights stay in T. The Float32
+ * solve then follows the Float64 one to round-off (3.6e-7 at that size) and
+ * no longer matches the reference's Float32 arithmetic (the cell list and its
+ * permutation are unchanged). No reference counterpart.
  * The mode applies to every later call on the handle (the environment
- * variable FFCM_STENCIL_OFFSETS=compensated sets it at ffcm_create); changing
- * it waits for the handle's stream and drops a pending adjoint checkpoint. */
-#define FFCM_OFFSETS_REFERENCE 0
-#define FFCM_OFFSETS_COMPENSATED 1
-int ffcm_set_stencil_offsets(ffcm_handle* h, int32_t mode);
-int ffcm_get_stencil_offsets(const ffcm_handle* h, int32_t* mode);
+ * variable FFCM_STENCIL=float64 sets it at ffcm_create); changing it waits for
+ * the handle's stream and drops a pending adjoint checkpoint. */
+#define FFCM_STENCIL_REFERENCE 0
+#define FFCM_STENCIL_FLOAT64 1
+int ffcm_set_stencil(ffcm_handle* h, int32_t mode);
+int ffcm_get_stencil(const ffcm_handle* h, int32_t* mode);
 
 /* Particle count, element type and cell count of a handle. */
 int ffcm_get_info(const ffcm_handle* h, int64_t* N, int32_t* dtype, int64_t* num_cells_total);

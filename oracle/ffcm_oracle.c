@@ -19,12 +19,22 @@
 #define PI_D 3.14159265358979323846
 
 /* Float32 instantiation. T(π) in Julia is Float32(π), the rounding of π. */
+/* Stencil geometry (a test option, not the reference): 0 selects the
+ * reference's arithmetic in the working precision; otherwise the double
+ * spacing hd of the box as the caller gave it: anchors rounded from
+ * Y * (1 / hd) in double, offsets fma(g, h_hi, -Y) + g h_lo with
+ * h_hi + h_lo = hd in the working precision (the library's
+ * FFCM_STENCIL_FLOAT64 mode). */
+static double g_geom_hd = 0.0;
+void oracle_set_stencil_geometry(double hd) { g_geom_hd = hd; }
+
 #define FT float
 #define SFX _f
 #define FMOD fmodf
 #define COPYSIGN copysignf
 #define FLOOR floorf
 #define RINT rintf
+#define FMA fmaf
 #define EXP expf
 #define SQRT sqrtf
 #define POW powf
@@ -37,6 +47,7 @@
 #undef COPYSIGN
 #undef FLOOR
 #undef RINT
+#undef FMA
 #undef EXP
 #undef SQRT
 #undef POW
@@ -50,6 +61,7 @@
 #define COPYSIGN copysign
 #define FLOOR floor
 #define RINT rint
+#define FMA fma
 #define EXP exp
 #define SQRT sqrt
 #define POW pow

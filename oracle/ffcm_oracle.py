@@ -147,9 +147,15 @@ class OracleConfig:
     """
 
     def __init__(self, T, *, L, R_c, N, a=None, kernel_widths_ratio, num_grid_points, M_G,
-                 viscosity, fft_planning="measure", fft_threads=1):
+                 viscosity, fft_planning="measure", fft_threads=1, stencil="reference"):
         T = np.dtype(T).type
         self.T = T
+        # stencil geometry: "reference" (the reference's arithmetic in T) or
+        # "float64" (not the reference: anchors and offsets from the double
+        # spacing of the box as given, the library's FFCM_STENCIL_FLOAT64)
+        if stencil not in ("reference", "float64"):
+            raise ValueError(f"stencil must be 'reference' or 'float64'; got {stencil!r}")
+        self.stencil_hd = float(L[0]) / int(num_grid_points[0]) if stencil == "float64" else 0.0
         L = tuple(T(x) for x in L)
         R_c = T(R_c)
         a = T(1) if a is None else T(a)
@@ -279,8 +285,14 @@ def modified_kernel_coefficients(sigma, Sigma):
     return tuple(T(x) for x in out)
 
 
+def _geometry(cfg):
+    """Select the configuration's stencil geometry in the C oracle."""
+    lib().oracle_set_stencil_geometry(ctypes.c_double(getattr(cfg, "stencil_hd", 0.0)))
+
+
 def spread_forces(cfg):
     """src/spread_forces.jl:17-33 / 73-130: overwrite cfg.force_density."""
+    _geometry(cfg)
     T = cfg.T
     ct = _ct(T)
     getattr(lib(), "oracle_spread" + _sfx(T))(
@@ -328,6 +340,7 @@ def stokes_solve(cfg):
 
 def interpolate_velocities(V, cfg):
     """src/interpolate.jl:23-42 / 322-376: V[:, original_index[s]] = h^3 * v."""
+    _geometry(cfg)
     T = cfg.T
     ct = _ct(T)
     getattr(lib(), "oracle_interpolate" + _sfx(T))(
@@ -435,6 +448,7 @@ def adjoint(cfg, Y, F, lam):
     correct_velocities(dF, cfg)
     cfg.F_sorted[...] = F_sorted
     dY = np.zeros((N, 3), T)
+    _geometry(cfg)
     getattr(lib(), "oracle_grad_gather" + _sfx(T))(
         _p(dY), _p(u), _p(psi), _p(cfg.Y_sorted), _p(F_sorted), _p(L_sorted),
         _p(cfg.original_index), ctypes.c_int64(N), ct(cfg.sigma), ct(cfg.Sigma), ct(cfg.h),

@@ -75,17 +75,32 @@ void FN(oracle_modified_kernel_coefficients)(FT sigma, FT Sigma, FT* out4) {
     out4[0] = a0; out4[1] = a2; out4[2] = inv_norm; out4[3] = inv_2S2;
 }
 
+/* Anchor round(Y / h) and offset g h - Y of the stencil (src/stencil.jl:97-105),
+ * or the Float64 geometry when g_geom_hd is set (see ffcm_oracle.c). */
+static int32_t FN(stencil_anchor)(FT y, FT inv_h) {
+    if (g_geom_hd > 0) return (int32_t)rint((double)y * (1.0 / g_geom_hd));
+    return (int32_t)RINT(y * inv_h);
+}
+static FT FN(stencil_offset)(int32_t gi, FT y, FT h) {
+    if (g_geom_hd > 0) {
+        const FT hh = (FT)g_geom_hd;
+        const FT hl = (FT)(g_geom_hd - (double)hh);
+        return FMA((FT)gi, hh, -y) + (FT)gi * hl;
+    }
+    return (FT)gi * h - y;
+}
+
 /* src/stencil.jl:80-112  _fill_particle_stencil! for one particle.
  * g[axis*MG+k], r2[axis*MG+k], idx[axis*MG+k] (0-based wrapped index). */
 static void FN(fill_stencil)(FT* g, FT* r2, int32_t* idx, const FT* Y, FT inv_norm,
                             FT inv_2S2, FT h, FT inv_h, const int32_t* M, int32_t MG) {
     int32_t half = MG / 2;
     for (int i = 0; i < 3; ++i) {
-        int32_t j = (int32_t)RINT(Y[i] * inv_h);
+        int32_t j = FN(stencil_anchor)(Y[i], inv_h);
         for (int32_t k = 1; k <= MG; ++k) {
             int32_t off = k - 1 - half;
             int32_t gi = j + off;
-            FT x = (FT)gi * h - Y[i];
+            FT x = FN(stencil_offset)(gi, Y[i], h);
             FT x2 = x * x;
             g[i * MG + k - 1] = inv_norm * (FT)EXP(-x2 * inv_2S2);
             r2[i * MG + k - 1] = x2;
@@ -375,8 +390,8 @@ void FN(oracle_grad_gather)(FT* dY, const FT* u, const FT* psi, const FT* Y_sort
         const FT* Ln = L_sorted + 3 * s;
         FN(fill_stencil)(g, r2, idx, Yn, inv_norm, inv_2S2, h, inv_h, M, MG);
         for (int i = 0; i < 3; ++i) {
-            int32_t j = (int32_t)RINT(Yn[i] * inv_h);
-            for (int32_t k = 0; k < MG; ++k) xo[i * MG + k] = (FT)(j + k - half) * h - Yn[i];
+            int32_t j = FN(stencil_anchor)(Yn[i], inv_h);
+            for (int32_t k = 0; k < MG; ++k) xo[i * MG + k] = FN(stencil_offset)(j + k - half, Yn[i], h);
         }
         FT d0 = 0, d1 = 0, d2 = 0;
         for (int32_t kz = 0; kz < MG; ++kz)

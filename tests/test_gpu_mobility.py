@@ -211,18 +211,20 @@ def test_n500k_512_against_oracle(ffcm, n500k_inputs):
     o64 = O.OracleConfig(np.float64, **kw)
     o64.fft_threads = 8
     V64 = O.apply(o64, Y32.astype(np.float64), F32.astype(np.float64))
-    # With the reference's Float32 offsets g*h - Y (two numbers near
-    # L = 275.6 cancel) the Float32 algorithm itself sits ~2.2e-4 from
-    # Float64; the default mode reproduces it (parity above), and the
-    # compensated offsets bring the same Float32 solve under 1e-4 of Float64.
+    # With the reference's Float32 anchors round(Y / h), the few particles
+    # whose Y / h sits within Float32 rounding of a half-integer take a
+    # neighbouring truncated stencil, and the Float32 algorithm itself sits
+    # 2.2e-4 from Float64; the default mode reproduces it (parity above), and
+    # Float64 stencil geometry brings the same Float32 solve to the Float64
+    # answer (the oracle's own Float32 run with that geometry: 3.6e-7).
     err_reference = rel_l2(Vg, V64)
-    prod.stencil_offsets = "compensated"
+    prod.stencil = "float64"
     Vc = _run(ffcm, prod, Y32, F32)
     assert np.array_equal(prod.original_index, o32.original_index)   # same cell list
-    err_compensated = rel_l2(Vc, V64)
-    print(f"N=500k 512^3 F32 vs F64 oracle: reference offsets {err_reference:.3e}, "
-          f"compensated offsets {err_compensated:.3e}")
-    assert err_compensated < 1e-4
+    err_float64 = rel_l2(Vc, V64)
+    print(f"N=500k 512^3 F32 vs F64 oracle: reference stencil {err_reference:.3e}, "
+          f"Float64 stencil geometry {err_float64:.3e}")
+    assert err_float64 < 1e-5
 
 
 def test_n500k_512_properties(ffcm, n500k_inputs):
@@ -384,53 +386,77 @@ def test_fixed_position_operator_on_cuda_tensors(ffcm, T):
     assert rel_l2(V_dd.cpu().numpy(), V_host) < bound
 
 
-# ---- compensated stencil offsets (no reference counterpart) ----------------
+# ---- Float64 stencil geometry (no reference counterpart) -------------------
 @pytest.mark.parametrize("name", ["uniform_N2000_64", "standard_random256"])
-def test_compensated_offsets_follow_float64(ffcm, name):
-    """The opt-in compensated offset keeps the cell list and moves the Float32
-    solve toward the Float64 answer; the default stays at reference parity."""
+def test_float64_stencil_follows_float64(ffcm, name):
+    """The opt-in Float64 stencil geometry keeps the cell list, matches the
+    oracle run with the same geometry, and moves the Float32 solve to the
+    Float64 answer; the default stays at reference parity."""
     z = np.load(GOLDEN / f"{name}.npz")
     Lb, N, M, MG, Rc, ratio = z["meta"]
     kw = kw_of(Lb, int(N), int(M), M_G=int(MG), R_c=Rc, ratio=ratio)
     ref_cfg = ffcm.FFCMConfig(np.float32, **kw)
-    assert ref_cfg.stencil_offsets == "reference"
-    comp = ffcm.FFCMConfig(np.float32, stencil_offsets="compensated", **kw)
-    assert comp.stencil_offsets == "compensated"
+    assert ref_cfg.stencil == "reference"
+    geo = ffcm.FFCMConfig(np.float32, stencil="float64", **kw)
+    assert geo.stencil == "float64"
     Vr = _run(ffcm, ref_cfg, z["f32_Y"], z["f32_F"])
-    Vc = _run(ffcm, comp, z["f32_Y"], z["f32_F"])
-    assert np.array_equal(comp.original_index, z["f32_original_index"])
+    Vg = _run(ffcm, geo, z["f32_Y"], z["f32_F"])
+    assert np.array_equal(geo.original_index, z["f32_original_index"])
     assert rel_l2(Vr, z["f32_V"]) < 1e-5
+    ora = O.OracleConfig(np.float32, stencil="float64", **kw)
+    assert rel_l2(Vg, O.apply(ora, z["f32_Y"], z["f32_F"])) < 1e-5
     V64 = z["f64_V"]
-    e_ref, e_comp = rel_l2(Vr, V64), rel_l2(Vc, V64)
-    assert e_comp < 1e-5 and e_comp <= e_ref
+    assert rel_l2(Vg, V64) < 1e-5 and rel_l2(Vg, V64) <= rel_l2(Vr, V64) * 1.01
     # Float64 handles take the mode too and stay at Float64 accuracy
-    c64 = ffcm.FFCMConfig(np.float64, stencil_offsets="compensated", **kw)
+    c64 = ffcm.FFCMConfig(np.float64, stencil="float64", **kw)
     assert rel_l2(_run(ffcm, c64, z["f64_Y"], z["f64_F"]), V64) < 1e-10
 
 
-def test_compensated_offsets_switch_on_a_live_configuration(ffcm):
+def test_float64_stencil_slab_and_generic_paths(ffcm):
+    """Both the fused slab kernels and the generic step kernels take the
+    Float64 geometry, on a box whose length Float32 cannot represent."""
+    L, M, N = (27.3, 27.3, 27.3), (64, 64, 64), 3000
+    kw = dict(L=L, R_c=3.0, N=N, kernel_widths_ratio=2.0, viscosity=1.0, num_grid_points=M, M_G=8)
+    Y, F = random_cloud(np.float32, N, L, 77)
+    ora = O.OracleConfig(np.float32, stencil="float64", **kw)
+    Vo = O.apply(ora, Y, F)
+    fused = ffcm.FFCMConfig(np.float32, stencil="float64", **kw)
+    assert rel_l2(_run(ffcm, fused, Y, F), Vo) < 1e-5
+    steps = ffcm.FFCMConfig(np.float32, stencil="float64", **kw)
+    ffcm.wrap_positions(steps, Y)
+    ffcm.assign_cells(steps)
+    ffcm.sort_particles_by_cell(steps, F)
+    ffcm.spread_forces(steps)
+    ffcm.stokes_solve(steps)
+    V = np.zeros_like(Y)
+    ffcm.interpolate_velocities(V, steps)
+    ffcm.correct_velocities(V, steps)
+    assert rel_l2(V, Vo) < 1e-5
+
+
+def test_float64_stencil_switch_on_a_live_configuration(ffcm):
     """Switching the mode applies to the next call, drops a pending adjoint
     checkpoint, and rebuilds the conjugate-gradient graph."""
     z = np.load(GOLDEN / "uniform_N2000_64.npz")
     Y, F = z["f32_Y"], z["f32_F"]
     kw = kw_of(40.0, 2000, 64, R_c=3.0)
     cfg = ffcm.FFCMConfig(np.float32, **kw)
-    ref = ffcm.FFCMConfig(np.float32, stencil_offsets="compensated", **kw)
+    ref = ffcm.FFCMConfig(np.float32, stencil="float64", **kw)
     Vref = _run(ffcm, ref, Y, F)
     V = np.empty_like(Y)
     ffcm.mobility_checkpoint(V, cfg, Y, F)
-    cfg.stencil_offsets = "compensated"
+    cfg.stencil = "float64"
     with pytest.raises(ffcm.FFCMError):
         ffcm.adjoint(np.empty_like(Y), np.empty_like(Y), cfg, V)
     assert rel_l2(_run(ffcm, cfg, Y, F), Vref) < 1e-6
     M = ffcm.FFCMMobility(cfg, Y)
     Fs, hist = ffcm.cg(M, V, log=True)
-    cfg.stencil_offsets = "reference"
+    cfg.stencil = "reference"
     Fs2, hist2 = ffcm.cg(M, V, log=True)
     assert hist.isconverged and hist2.isconverged
-    assert rel_l2(Fs2, Fs) < 1e-2          # different operators, nearby solutions
+    assert rel_l2(Fs2, Fs) < 1e-2          # nearby operators, nearby solutions
     with pytest.raises(ffcm.ArgumentError):
-        cfg.stencil_offsets = "fast"
+        cfg.stencil = "fast"
 
 
 def test_host_pointer_passed_as_device_memory_is_rejected(ffcm):
