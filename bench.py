@@ -331,7 +331,7 @@ def secondary_workloads(args, local_rank):
                     "gradient_step_cost_vs_forward", "e2e", "roofline", "pullback_stage_ms", "clocks",
                     "gpu_launches"),
         "clustered": ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config",
-                      "fixed_position_operator_ms_per_rhs", "gradient_ms_per_rhs", "stage_ms", "e2e",
+                      "fixed_position_operator_ms_per_rhs", "gradient_ms_per_rhs", "stage_ms", "tuning", "e2e",
                       "roofline", "clocks", "gpu_launches"),
     }
     runs = (("batched", measure_batched, 10), ("adjoint", measure_adjoint, 10), ("clustered", measure_clustered, 3))
@@ -400,6 +400,7 @@ def run_ours(args, rank, world, local_rank):
         barrier()
     launches = cfg.launch_count() - launches0
     ms = e0.elapsed_time(e1) / args.steps
+    tuning = cfg.tuning()
 
     # ---- per-stage CUDA events over a second timed pass ----------------------
     cfg.profile_begin()
@@ -480,6 +481,7 @@ def run_ours(args, rank, world, local_rank):
                                "achieved_GBs": solve_bytes / (ms / 1e3) / 1e9,
                                "frac": solve_bytes / (ms / 1e3) / 1e9 / peak},
             "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "tuning": tuning,
             "cpu_baseline": cpu,
             "accuracy": accuracy,
             "clocks": clk.summary(),
@@ -930,6 +932,7 @@ def measure_clustered(args, rank, world, local_rank):
     plain()
     torch.cuda.synchronize(dev)
     stages = cfg.profile_end()
+    tuning = cfg.tuning()
 
     def apply_all():
         assert lib.ffcm_set_positions(cfg.handle, ctypes.c_void_p(Yd.data_ptr()), 1, sh) == 0
@@ -976,6 +979,7 @@ def measure_clustered(args, rank, world, local_rank):
             "fixed_position_operator_ms_per_rhs": ms_apply / c["nrhs"],
             "gradient_ms_per_rhs": ms_grad / c["nrhs"],
             "stage_ms": stage_ms,
+            "tuning": tuning,
             "e2e": {"value": world * N / (ms_e2e / 1e3), "unit": "particles/s", "ms_per_step": ms_e2e,
                     "h2d_bytes_per_step": int(Yh.numel() * 8), "d2h_bytes_per_step": int(Vh.numel() * 4)},
             "cpu_baseline": None,

@@ -411,7 +411,6 @@ struct Engine final : EngineBase {
     // slab kernels: spread/interpolation fused with the x transforms
     bool slab = false;
     SlabKernels<T> sk;
-    int spread_kind = 0;   // FFCM_SPREAD: 0 tile owner, 1 pairs
     SlabGeom sg;
     T* partial = nullptr;
     int* slab_lists = nullptr;   // per-slab particle lists kept by the spread
@@ -574,16 +573,6 @@ struct Engine final : EngineBase {
             sg.lcap = (int)std::min<double>(1 << 20, std::max(256.0, 4.0 * expect + 64.0));
             sg.lcap = (sg.lcap + 31) / 32 * 32;
             TRY(raise_smem_cap((const void*)sk.spread_fused, sk.smem));
-            TRY(raise_smem_cap((const void*)sk.spread_pp, sk.smem_pp));
-            {
-                // spread window processing: 0 = per grid point (tile owner,
-                // deterministic), 1 = per (entry, x offset) pair with
-                // shared-memory atomics
-                const char* v = std::getenv("FFCM_SPREAD");
-                if (v && std::strcmp(v, "tile") == 0) spread_kind = 0;
-                else if (v && std::strcmp(v, "pairs") == 0) spread_kind = 1;
-                else if (v && *v) return fail(FFCM_ERR_ARGUMENT, "FFCM_SPREAD must be \"tile\" or \"pairs\"");
-            }
             TRY(raise_smem_cap((const void*)sk.interp, sk.smem_interp));
         }
         if (fast_y) {
@@ -1003,8 +992,7 @@ struct Engine final : EngineBase {
             TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
                        slab_lists, slab_counts));
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, spread_kind == 1 ? sk.spread_pp : sk.spread_fused, g, 256,
-                      spread_kind == 1 ? sk.smem_pp : sk.smem, s, (const vec4<T>*)Ys,
+        return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys,
                       force ? force : (const vec4<T>*)Fs,
                       (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, (const int*)slab_lists,
                       (const int*)slab_counts);

@@ -543,153 +543,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
     slab_x_r2c<T, H, BY, BZ>(acc, spec, hxp, p, tw, dummy, y0r, z0r);
 }
 
-// ---- spread by (entry, x offset) pairs with shared-memory atomics ------------
-// The same slab, window and x transform as k_spread_slab, with the window
-// processed pair-parallel instead of per grid point: the window's entries are
-// not ordered; lane q of a block round takes entry q / M_G and stencil x point
-// q % M_G (the 8 lanes of an entry are consecutive, so a warp serves 4 entries
-// and its lanes write 4 runs of 8 consecutive x), evaluates gx once and adds
-// F (a0 + a2 r^2) gx gy gz to every slab row the entry reaches with a
-// shared-memory float atomic. Every lane does the same amount of work (no
-// search for the entries covering an x, no window sort); the slab starts at
-// zero and the order of the additions is not fixed, so results may differ
-// from run to run in the last bits (as the reference's own GPU spread,
-// ext/ForceCouplingMethodCUDAExt/spread_forces.jl:139-171).
-template <typename T, int BY, int BZ>
-struct SpreadWinPP {
-    static constexpr int NRP = BY * BZ;
-    unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15) | first x + 32768 (16..31)
-    T y0[SLAB_CAP];
-    T f[3][SLAB_CAP];
-    // padded by one element: the 4 entries of a warp read different banks
-    T gyz[SLAB_CAP][NRP + 1], dyz[SLAB_CAP][NRP + 1];   // gy gz and gy gz (r2y + r2z)
-    int scan[32];
-};
-
-template <typename T, int BY, int BZ, int H>
-__host__ __device__ constexpr size_t spread_pp_win_bytes() {
-    return ((sizeof(SpreadWinPP<T, BY, BZ>) > (size_t)padded_len(H) * sizeof(cplx<T>)
-                 ? sizeof(SpreadWinPP<T, BY, BZ>)
-                 : (size_t)padded_len(H) * sizeof(cplx<T>)) + 15) / 16 * 16;
-}
-
-template <typename T, int BY, int BZ>
-__device__ __forceinline__ void spread_put_pp(const StencilParams<T>& p, SpreadWinPP<T, BY, BZ>& W, int i,
-                                              const vec4<T>& y, const vec4<T>& f, int sx, int sy, int sz,
-                                              unsigned m, int y0r, int z0r) {
-    constexpr int NRP = BY * BZ;
-    W.msk[i] = m | ((unsigned)(sx + 32768) << 16);   // the stencil's first x point, offset into bits 16..31
-    W.y0[i] = y.x;
-    W.f[0][i] = f.x;
-    W.f[1][i] = f.y;
-    W.f[2][i] = f.z;
-    T gyz[NRP], r2yz[NRP];
-    row_weights<T, BY, BZ>(p, y, sy, sz, m, y0r, z0r, gyz, r2yz);
-#pragma unroll
-    for (int r = 0; r < NRP; ++r) {
-        W.gyz[i][r] = gyz[r];
-        W.dyz[i][r] = gyz[r] * r2yz[r];
-    }
-}
-
-template <typename T, int H, int BY, int BZ>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab_pp(const vec4<T>* __restrict__ Ys,
-                                                        const vec4<T>* __restrict__ Fs,
-                                                        const int32_t* __restrict__ off,
-                                                        cplx<T>* __restrict__ spec, int hxp,
-                                                        StencilParams<T> p, SlabGeom g,
-                                                        const cplx<T>* __restrict__ twx,
-                                                        const int* __restrict__ lists,
-                                                        const int* __restrict__ counts) {
-    constexpr int Mx = 2 * H, P = slab_pitch(Mx), NRP = BY * BZ, ROWS = 3 * NRP;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T* acc = reinterpret_cast<T*>(smem_raw);
-    SpreadWinPP<T, BY, BZ>& W = *reinterpret_cast<SpreadWinPP<T, BY, BZ>*>(acc + ROWS * P);
-    cplx<T>* dummy = reinterpret_cast<cplx<T>*>(&W);   // idle-lane FFT line: the window is dead by then
-    cplx<T>* tw = reinterpret_cast<cplx<T>*>(reinterpret_cast<unsigned char*>(&W) +
-                                             spread_pp_win_bytes<T, BY, BZ, H>());
-    load_table(tw, twx, Mx);
-    for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
-    const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
-    const int cta = blockIdx.x + blockIdx.y * gridDim.x;
-    // entries [0, count) are in W; all threads call this after a barrier
-    auto process = [&](int count) {
-        for (int q = threadIdx.x; q < count * SLAB_MG; q += blockDim.x) {
-            const int i = q / SLAB_MG, e = q % SLAB_MG;
-            const unsigned m = W.msk[i];
-            const int gx = (int)(m >> 16) - 32768 + e;   // stencil x point (unwrapped)
-            T gxe, r2xe;
-            axis_weight(p, gx, W.y0[i], gxe, r2xe);
-            // (a0 + a2 (r2x + r2yz)) gx gyz = [gx (a0 + a2 r2x)] gyz + [a2 gx] [gyz r2yz]
-            const T wa = gxe * (p.a0 + p.a2 * r2xe), wc = p.a2 * gxe;
-            const T f0 = W.f[0][i], f1 = W.f[1][i], f2 = W.f[2][i];
-            T* ax = acc + wrap1(gx, Mx);
-#pragma unroll
-            for (int d = 0; d < BZ; ++d)
-#pragma unroll
-                for (int b = 0; b < BY; ++b) {
-                    if (!((m >> b) & (m >> (8 + d)) & 1u)) continue;
-                    const int r = d * BY + b;
-                    const T wgt = wa * W.gyz[i][r] + wc * W.dyz[i][r];
-                    atomicAdd(ax + r * P, wgt * f0);
-                    atomicAdd(ax + (NRP + r) * P, wgt * f1);
-                    atomicAdd(ax + (2 * NRP + r) * P, wgt * f2);
-                }
-        }
-    };
-    __syncthreads();   // the slab is zero
-    const int stored = counts[cta];
-    if (stored >= 0) {
-        const int* glist = lists + (int64_t)cta * g.lcap;
-        for (int w0 = 0; w0 < stored; w0 += SLAB_CAP) {
-            const int n = min(SLAB_CAP, stored - w0);
-            if ((int)threadIdx.x < n) {
-                const int s = glist[w0 + threadIdx.x];
-                const vec4<T> y = Ys[s];
-                int sx, sy, sz;
-                unsigned m;
-                slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
-                spread_put_pp<T, BY, BZ>(p, W, (int)threadIdx.x, y, Fs[s], sx, sy, sz, m, y0r, z0r);
-            }
-            __syncthreads();
-            process(n);
-            __syncthreads();
-        }
-    } else {
-        // the list overflowed: scan the candidates in chunks of SLAB_CAP and
-        // compact the touching ones into windows, in candidate order
-        const SlabRows rows = slab_rows<BY, BZ>(g, y0r, z0r);
-        int count = 0;
-        for (int pi = 0; pi < rows.ny * rows.nz; ++pi) {
-            const int c0 = slab_row_cell(g, rows, pi);
-            const int sb = off[c0], se = off[c0 + g.m0];
-            for (int b = sb; b < se; b += SLAB_CAP) {
-                const int s = b + (int)threadIdx.x;
-                unsigned m = 0;
-                int sx = 0, sy = 0, sz = 0;
-                vec4<T> y{};
-                if ((int)threadIdx.x < SLAB_CAP && s < se) {
-                    y = Ys[s];
-                    slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
-                }
-                int tot;
-                const int pre = block_scan(m ? 1 : 0, W.scan, tot);
-                if (count + tot > SLAB_CAP) {   // block-uniform
-                    process(count);
-                    __syncthreads();
-                    count = 0;
-                }
-                if (m) spread_put_pp<T, BY, BZ>(p, W, count + pre, y, Fs[s], sx, sy, sz, m, y0r, z0r);
-                count += tot;
-                __syncthreads();
-            }
-        }
-        if (count > 0) process(count);
-        __syncthreads();
-    }
-    slab_x_r2c<T, H, BY, BZ>(acc, spec, hxp, p, tw, dummy, y0r, z0r);
-}
-
 // ---- x-c2r of a slab into shared memory, then gather partial velocities ----
 // Each slab adds its partial sums into Vs[3 s + c] (sorted order, zeroed
 // beforehand); the correction kernel finishes V[:, perm[s]] = h^3 Vs[s] + dv.
@@ -753,61 +606,6 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
         }
         return true;
     };
-    // While the rows land: order the slab's listed particles so that the 32
-    // lanes of a warp gather from different shared-memory banks. With one
-    // thread per particle, lane i reads row[x0_i + e] for every stencil point
-    // e; lanes whose first x points differ mod 32 read distinct banks. The
-    // entries are bucketed by x0 mod 32 and dealt out round-robin over the
-    // buckets (the k-th entry of every non-empty bucket, then the (k+1)-th, ...),
-    // so 32 consecutive entries share a bank at most twice. The order changes
-    // which thread sums a particle, not the sum.
-    constexpr int ICAP = 512;   // entries ordered this way (longer lists keep their order)
-    __shared__ int s_ord[ICAP];
-    __shared__ int s_base[ICAP];
-    __shared__ unsigned s_mk[ICAP];
-    __shared__ int s_cnt[32];
-    const int stored = counts[cta];
-    const bool reorder = stored > 0 && stored <= ICAP && blockDim.x * 2 >= ICAP;
-    if (reorder) {
-        const int* glist = lists + (int64_t)cta * g.lcap;
-        if (threadIdx.x < 32) s_cnt[threadIdx.x] = 0;
-        __syncthreads();
-        int res[2], rk[2], ss[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            const int t = (int)threadIdx.x + u * (int)blockDim.x;
-            res[u] = -1;
-            rk[u] = 0;
-            ss[u] = 0;
-            if (t < stored) {
-                ss[u] = glist[t];
-                const int x0 = wrap1(stencil_anchor(p, Ys[ss[u]].x) - SLAB_MG / 2, Mx);
-                res[u] = x0 & 31;
-                rk[u] = atomicAdd(&s_cnt[res[u]], 1);
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            const int c = s_cnt[threadIdx.x];
-            int kmax = c;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-            int base = 0;
-            for (int k = 0; k < kmax; ++k) {   // kmax <= stored <= ICAP
-                const unsigned mk = __ballot_sync(0xffffffffu, c > k);
-                if (threadIdx.x == 0) {
-                    s_base[k] = base;
-                    s_mk[k] = mk;
-                }
-                base += __popc(mk);
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int u = 0; u < 2; ++u)
-            if (res[u] >= 0) s_ord[s_base[rk[u]] + __popc(s_mk[rk[u]] & ((1u << res[u]) - 1u))] = ss[u];
-        // read by the gather after the barrier that ends the x transforms
-    }
     if (!landed(0)) return;
     if constexpr (R16) {
         // x lengths 128..512: L = H / 16 threads per row (see the spread)
@@ -918,9 +716,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
         atomicAdd(vs + 1, v1);
         atomicAdd(vs + 2, v2);
     };
+    const int stored = counts[cta];
     if (stored >= 0) {
         const int* glist = lists + (int64_t)cta * g.lcap;
-        for (int t = threadIdx.x; t < stored; t += blockDim.x) gather(reorder ? s_ord[t] : glist[t]);
+        for (int t = threadIdx.x; t < stored; t += blockDim.x) gather(glist[t]);
     } else {
         // the list overflowed: every candidate of the slab's cell rows
         const SlabRows rows = slab_rows<BY, BZ>(g, y0r, z0r);
@@ -945,8 +744,6 @@ using InterpSlabKernel = void (*)(const vec4<T>*, const int32_t*, const cplx<T>*
 template <typename T>
 struct SlabKernels {
     SpreadSlabKernel<T> spread_fused = nullptr;
-    SpreadSlabKernel<T> spread_pp = nullptr;   // pair-parallel window processing
-    size_t smem_pp = 0;
     InterpSlabKernel<T> interp = nullptr;
     ListsKernel<T> lists = nullptr;
     int BY = 0, BZ = 0;
@@ -959,7 +756,6 @@ SlabKernels<T> slab_kernels_for() {
     constexpr int BY = SlabShape<T, H>::BY, BZ = SlabShape<T, H>::BZ;
     SlabKernels<T> k;
     k.spread_fused = k_spread_slab<T, H, BY, BZ>;
-    k.spread_pp = k_spread_slab_pp<T, H, BY, BZ>;
     k.interp = k_interp_slab<T, H, BY, BZ>;
     k.lists = k_slab_lists<T, BY, BZ>;
     k.BY = BY;
@@ -968,7 +764,6 @@ SlabKernels<T> slab_kernels_for() {
     const size_t line_bytes = (size_t)padded_len(H) * sizeof(cplx<T>);
     const size_t table_bytes = (size_t)2 * H * sizeof(cplx<T>);
     k.smem = slab_bytes + spread_win_bytes<T, BY, BZ, H>() + table_bytes;
-    k.smem_pp = slab_bytes + spread_pp_win_bytes<T, BY, BZ, H>() + table_bytes;
     k.smem_interp = slab_bytes + line_bytes + table_bytes;
     return k;
 }
