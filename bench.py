@@ -348,14 +348,7 @@ def secondary_workloads(args, local_rank):
 
 def run_ours(args, rank, world, local_rank):
     import torch
-    import importlib.util
-
-    pkg = ROOT / "ffcm.jl_b200"
-    spec = importlib.util.spec_from_file_location("ffcm_b200", pkg / "__init__.py",
-                                                  submodule_search_locations=[str(pkg)])
-    ffcm = importlib.util.module_from_spec(spec)
-    sys.modules["ffcm_b200"] = ffcm
-    spec.loader.exec_module(ffcm)
+    ffcm = _load_product()
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -589,15 +582,8 @@ def batched_checksum(results):
 
 def measure_batched(args, rank, world, local_rank):
     import torch
-    import importlib.util
     from fixtures import nonoverlapping_uniform
-
-    pkg = ROOT / "ffcm.jl_b200"
-    spec = importlib.util.spec_from_file_location("ffcm_b200", pkg / "__init__.py",
-                                                  submodule_search_locations=[str(pkg)])
-    ffcm = importlib.util.module_from_spec(spec)
-    sys.modules["ffcm_b200"] = ffcm
-    spec.loader.exec_module(ffcm)
+    ffcm = _load_product()
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     dist = None
@@ -901,7 +887,7 @@ def measure_clustered(args, rank, world, local_rank):
         Vts.append(vt)
     stream = torch.cuda.current_stream(dev)
     sh = ctypes.c_void_p(stream.cuda_stream or 1)
-    lib = ffcm._lib.load()
+    lib = ffcm.L_.load()
 
     def barrier():
         torch.cuda.synchronize(dev)

@@ -992,7 +992,7 @@ struct Engine final : EngineBase {
             TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
                        slab_lists, slab_counts));
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys,
+        return launch(h, sk.spread_fused, g, sk.spread_threads, sk.smem, s, (const vec4<T>*)Ys,
                       force ? force : (const vec4<T>*)Fs,
                       (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, (const int*)slab_lists,
                       (const int*)slab_counts);
@@ -1030,7 +1030,7 @@ struct Engine final : EngineBase {
         StageScope sc(h, FFCM_STAGE_INTERPOLATE, s);
         CUDA_TRY(cudaMemsetAsync(partial, 0, 3 * (size_t)N * sizeof(T), s));
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, sk.interp, g, 256, sk.smem_interp, s, (const vec4<T>*)Ys, (const int32_t*)off,
+        return launch(h, sk.interp, g, sk.spread_threads, sk.smem_interp, s, (const vec4<T>*)Ys, (const int32_t*)off,
                       (const cplx<T>*)spec, hxp, partial, sp, sg, (const cplx<T>*)twx,
                       (const int*)slab_lists, (const int*)slab_counts, h->d_err);
     }
