@@ -601,6 +601,8 @@ struct Engine final : EngineBase {
                 TRY(raise_smem_cap((const void*)ytma_kernel<T>(My, B), ytma_smem<T>(My, B)));
             if (fast_z && ztma_kernel<T>(Mz, B) && ztma_smem<T>(Mz, B) <= 226 * 1024)
                 TRY(raise_smem_cap((const void*)ztma_kernel<T>(Mz, B), ztma_smem<T>(Mz, B)));
+            if (fast_z && zin_kernel<T>(Mz, B) && zin_smem<T>(Mz, B) <= 226 * 1024)
+                TRY(raise_smem_cap((const void*)zin_kernel<T>(Mz, B), zin_smem<T>(Mz, B)));
             if (fast_z && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= budget)
                 TRY(raise_smem_cap((const void*)zlr_kernel<T>(Mz, B), FastFft<T>::zlr_smem(Mz, B)));
             if (fast_z && zpipe_kernel<T>(Mz, B) && hxp % B == 0 && zpipe_smem<T>(Mz, B) <= budget)
@@ -737,7 +739,7 @@ struct Engine final : EngineBase {
         };
         for (int i = 1, B = 2; B <= 16; ++i, B *= 2) {
             if (hxp % B != 0) continue;
-            if (fast_z && ztma_kernel<T>(Mz, B))
+            if (fast_z && (ztma_kernel<T>(Mz, B) || zin_kernel<T>(Mz, B)))
                 zmap_ok[i] = make(&zmap[i], (cuuint32_t)(B * EPC), 1, (cuuint32_t)tma_zbox(Mz));
             if (fast_y && ytma_kernel<T>(My, B))
                 ymap_ok[i] = make(&ymap[i], (cuuint32_t)(B * EPC), (cuuint32_t)tma_zbox(My), 1);
@@ -781,7 +783,9 @@ struct Engine final : EngineBase {
                              zpipe_smem<T>(Mz, B) <= 200 * 1024 && t.zgrid >= 1) ||
                             (k == 2 && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= 200 * 1024) ||
                             (k == 3 && ztma_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
-                             ztma_smem<T>(Mz, B) <= 226 * 1024 && t.zgrid >= 1);
+                             ztma_smem<T>(Mz, B) <= 226 * 1024 && t.zgrid >= 1) ||
+                            (k == 4 && zin_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
+                             zin_smem<T>(Mz, B) <= 226 * 1024 && t.zgrid >= 1);
             if (!ok) return false;
         }
         // persistent grids are at most (blocks per SM) x SMs; anything larger
@@ -866,9 +870,11 @@ struct Engine final : EngineBase {
         if (fast_z) {
             float best = 1e30f;
             int bk = 0, bB = Bz, bg = 0;
-            for (int kind = 0; kind < 4; ++kind)
+            for (int kind = 0; kind < 5; ++kind)
                 for (int B : {2, 4, 8, 16}) {
                     if (fzk >= 0 && (kind != fzk || B != fzB)) continue;
+                    if (kind == 4 && !(zin_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
+                                       zin_smem<T>(Mz, B) <= 226 * 1024)) continue;
                     if (kind == 0 && !z_kernel<T>(Mz, B)) continue;
                     if (kind == 1 && !(zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
                                        zpipe_smem<T>(Mz, B) <= 200 * 1024)) continue;
@@ -893,6 +899,11 @@ struct Engine final : EngineBase {
                         const int ntiles = ((nkx + B - 1) / B) * My;
                         TRY(persistent_grid((const void*)ztma_kernel<T>(Mz, B), B * (Mz / 8),
                                             ztma_smem<T>(Mz, B), ntiles, zgrid));
+                    }
+                    if (kind == 4) {
+                        const int ntiles = ((nkx + B - 1) / B) * My;
+                        TRY(persistent_grid((const void*)zin_kernel<T>(Mz, B), B * (Mz / 8),
+                                            zin_smem<T>(Mz, B), ntiles, zgrid));
                     }
                     float ms = 0;
                     TRY(time_launches([&] { return launch_z(h->stream); }, ms));
@@ -992,7 +1003,7 @@ struct Engine final : EngineBase {
             TRY(launch(h, sk.lists, (nslab + 7) / 8, 256, 0, s, (const vec4<T>*)Ys, (const int32_t*)off, sp, sg,
                        slab_lists, slab_counts));
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, sk.spread_fused, g, sk.spread_threads, sk.smem, s, (const vec4<T>*)Ys,
+        return launch(h, sk.spread_fused, g, 256, sk.smem, s, (const vec4<T>*)Ys,
                       force ? force : (const vec4<T>*)Fs,
                       (const int32_t*)off, spec, hxp, sp, sg, (const cplx<T>*)twx, (const int*)slab_lists,
                       (const int*)slab_counts);
@@ -1030,7 +1041,7 @@ struct Engine final : EngineBase {
         StageScope sc(h, FFCM_STAGE_INTERPOLATE, s);
         CUDA_TRY(cudaMemsetAsync(partial, 0, 3 * (size_t)N * sizeof(T), s));
         dim3 g(sg.nty, sg.ntz, 1);
-        return launch(h, sk.interp, g, sk.spread_threads, sk.smem_interp, s, (const vec4<T>*)Ys, (const int32_t*)off,
+        return launch(h, sk.interp, g, 256, sk.smem_interp, s, (const vec4<T>*)Ys, (const int32_t*)off,
                       (const cplx<T>*)spec, hxp, partial, sp, sg, (const cplx<T>*)twx,
                       (const int*)slab_lists, (const int*)slab_counts, h->d_err);
     }
@@ -1204,6 +1215,12 @@ struct Engine final : EngineBase {
 
     int launch_z(cudaStream_t s, int k0 = 0, int k1 = 0) {
         if (k1 <= 0) k1 = nkx;
+        if (fast_z && zkind == 4) {
+            const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
+            return launch(h, zin_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), zin_smem<T>(Mz, Bz), s,
+                          zmap[log2i(Bz)], spec, k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv,
+                          (const T*)kyv, (const T*)kzv, inv_mu_M, h->d_err);
+        }
         if (fast_z && zkind == 3) {
             const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
             return launch(h, ztma_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), ztma_smem<T>(Mz, Bz), s,

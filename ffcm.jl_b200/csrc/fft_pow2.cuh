@@ -48,13 +48,23 @@ struct Exchange {
     __device__ __forceinline__ cplx<T>& at(int i) const { return sm[base + pad8(i) * es]; }
 };
 
+// Exchange through shared memory laid out densely: line b, element i at
+// sm[base(b) + i * es] (no padding: the exchange is the line's own storage).
+template <typename T>
+struct ExchangeDense {
+    cplx<T>* sm;
+    int base;
+    int es;
+    __device__ __forceinline__ cplx<T>& at(int i) const { return sm[base + i * es]; }
+};
+
 // In-register FFT of one line: v[q] = x[j + q n/8] on entry, X[j + q n/8] on exit.
 // `tw` holds W_n^t for t = e * tws (tws = table stride). All threads of the
 // block must call this together (it contains __syncthreads()). With
 // WARP = true every line lies inside one warp (n/8 <= 32 consecutive threads,
 // lines not shared between warps) and the exchanges only synchronise the warp.
-template <typename T, int n, bool WARP = false>
-__device__ __forceinline__ void fft_line_regs(cplx<T> (&v)[8], int j, const Exchange<T>& ex,
+template <typename T, int n, bool WARP = false, typename EX = Exchange<T>>
+__device__ __forceinline__ void fft_line_regs(cplx<T> (&v)[8], int j, const EX& ex,
                                               const cplx<T>* tw, int tws, bool inv) {
     static_assert(!WARP || n / 8 <= 32, "a warp-synchronised line must fit in one warp");
     constexpr int L2 = ilog2c(n);

@@ -157,6 +157,121 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_z_stokes(
     if (threadIdx.x == 0) bulk_wait_all();
 }
 
+// z pass + projector on wide tiles transformed in place. The passes above
+// keep a separate exchange region beside a staging buffer that is refilled
+// while they compute, which caps a tile at 8 kx columns at z length 512 and 4
+// at 1024: each z row of a tile is then a 64- or 32-byte piece of memory, and
+// at 32 bytes the pass reaches 1.2 TB/s. Here a tile of B columns (B = 16 at
+// 512: 128-byte pieces; B = 8 at 1024) is loaded by tiled bulk copies into
+// the staging buffer, and the three components are transformed one after the
+// other in that buffer (it is also their exchange space): forward, projector,
+// inverse, then tiled bulk stores. Loads are not overlapped with the block's
+// own compute (one tile buffer); one block per SM, other SMs interleave.
+// block = B * n/8 threads; smem: up to 128 bytes of alignment slack | staging
+// (3 n B, 128-byte aligned) | table (n).
+template <typename T, int n, int B>
+__global__ void __launch_bounds__(B * (n / 8)) k_fftr_z_stokes(
+    const __grid_constant__ CUtensorMap tmap, cplx<T>* __restrict__ spec, int kx0, int kx1, int My, int hxp,
+    const cplx<T>* __restrict__ twz, const T* __restrict__ kxv, const T* __restrict__ kyv,
+    const T* __restrict__ kzv, T inv_mu_M, int* __restrict__ err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar;
+    constexpr int Q = n / 8, ZB = tma_zbox(n), NCOPY = 3 * n / ZB;
+    constexpr unsigned TILE_BYTES = (unsigned)(3 * n * B * sizeof(cplx<T>));
+    cplx<T>* stage = reinterpret_cast<cplx<T>*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
+    cplx<T>* tw = stage + 3 * n * B;
+    load_table(tw, twz, n);
+    const int b = threadIdx.x % B, j = threadIdx.x / B;
+    const int tiles_x = (kx1 - kx0 + B - 1) / B;
+    const int ntiles = tiles_x * My;
+    if (threadIdx.x == 0) mbar_init(&bar, 1);
+    __syncthreads();
+    // component c of the tile: stage[(c n + z) B + b]
+    auto comp = [&](int c) { return ExchangeDense<T>{stage + c * n * B, b, B}; };
+    unsigned phase = 0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
+        const int tx = t % tiles_x, y = t / tiles_x;
+        if (threadIdx.x == 0) {
+            bulk_wait_read_all();       // the previous tile's stores have read the buffer
+            fence_proxy_async_smem();   // and so have the block's own accesses
+            mbar_arrive_expect(&bar, TILE_BYTES);
+#pragma unroll
+            for (int k = 0; k < NCOPY; ++k)
+                tma_load_3d(stage + k * ZB * B, &tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, y, k * ZB, &bar);
+        }
+        const bool landed = mbar_wait_bounded(&bar, phase, 1 << 22);
+        if (__syncthreads_or(!landed)) {
+            if (threadIdx.x == 0) {
+                atomicOr(err, DEVERR_COPY_TIMEOUT);
+                bulk_wait_all();
+            }
+            mbar_wait_bounded(&bar, phase, 1 << 22);
+            return;
+        }
+        // forward transforms, one component at a time, in place
+#pragma unroll 1
+        for (int c = 0; c < 3; ++c) {
+            const ExchangeDense<T> ex = comp(c);
+            cplx<T> v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = ex.at(j + q * Q);
+            fft_line_regs<T, n, false, ExchangeDense<T>>(v, j, ex, tw, 1, false);
+            __syncthreads();   // every exchange read of this component is done
+#pragma unroll
+            for (int q = 0; q < 8; ++q) ex.at(j + q * Q) = v[q];
+        }
+        __syncthreads();
+        // projector (I - k k^T / k^2) / (mu k^2 M), k = 0 -> 0
+        const int kx = kx0 + tx * B + b;
+        const T k1 = kx < kx1 ? kxv[kx] : T(0);
+        const T k2 = kyv[y];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int z = j + q * Q;
+            const T k3 = kzv[z];
+            const ExchangeDense<T> e0 = comp(0), e1 = comp(1), e2 = comp(2);
+            cplx<T> a = e0.at(z), bb = e1.at(z), cc = e2.at(z);
+            const T ksq = k1 * k1 + k2 * k2 + k3 * k3;
+            if (ksq == T(0)) {
+                a = bb = cc = cplx<T>{T(0), T(0)};
+            } else {
+                const T inv_k2 = T(1) / ksq;
+                const T sc = inv_mu_M * inv_k2;
+                const T dre = (k1 * a.x + k2 * bb.x + k3 * cc.x) * inv_k2;
+                const T dim = (k1 * a.y + k2 * bb.y + k3 * cc.y) * inv_k2;
+                a = cplx<T>{sc * (a.x - k1 * dre), sc * (a.y - k1 * dim)};
+                bb = cplx<T>{sc * (bb.x - k2 * dre), sc * (bb.y - k2 * dim)};
+                cc = cplx<T>{sc * (cc.x - k3 * dre), sc * (cc.y - k3 * dim)};
+            }
+            e0.at(z) = a;
+            e1.at(z) = bb;
+            e2.at(z) = cc;
+        }
+        __syncthreads();
+        // inverse transforms
+#pragma unroll 1
+        for (int c = 0; c < 3; ++c) {
+            const ExchangeDense<T> ex = comp(c);
+            cplx<T> v[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[q] = ex.at(j + q * Q);
+            fft_line_regs<T, n, false, ExchangeDense<T>>(v, j, ex, tw, 1, true);
+            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < 8; ++q) ex.at(j + q * Q) = v[q];
+        }
+        fence_proxy_async_smem();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < NCOPY; ++k)
+                tma_store_3d(&tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, y, k * ZB, stage + k * ZB * B);
+            bulk_commit();
+        }
+    }
+    if (threadIdx.x == 0) bulk_wait_all();
+}
+
 // y pass, same scheme: a tile is B kx columns x all n rows y of one (c, z)
 // plane (tensor coordinate z = c * Mz + z), loaded with n / min(256, n) tiled
 // copies into staging laid out [y][B].
@@ -254,6 +369,20 @@ using ZTmaKernel = void (*)(const CUtensorMap, cplx<T>*, int, int, int, int, con
 template <typename T>
 size_t ztma_smem(int n, int B) {
     return 128 + (size_t)(3 * n * B + n + 3 * B * padded_len(n)) * sizeof(cplx<T>);
+}
+
+template <typename T>
+size_t zin_smem(int n, int B) {
+    return 128 + (size_t)(3 * n * B + n) * sizeof(cplx<T>);
+}
+
+// In-place wide-tile z pass (k_fftr_z_stokes), per (n, B).
+template <typename T>
+ZTmaKernel<T> zin_kernel(int n, int B) {
+#define FFCM_ZI(NN, BB) if (n == NN && B == BB) return k_fftr_z_stokes<T, NN, BB>;
+    FFCM_ZI(256, 16) FFCM_ZI(512, 8) FFCM_ZI(512, 16) FFCM_ZI(1024, 8)
+#undef FFCM_ZI
+    return nullptr;
 }
 
 template <typename T>

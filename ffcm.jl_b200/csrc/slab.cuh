@@ -8,7 +8,7 @@
 // (cy, cz) rows of cells that can reach it, in cell-sorted order, with the
 // reference's integer anchor arithmetic).
 //
-//  * k_spread_slab: the list is replayed in windows of up to 256 entries; one
+//  * k_spread_slab: the list is replayed in windows of SLAB_CAP entries; one
 //    thread per entry stores the entry's per-row weights gy gz and r^2 parts
 //    (src/stencil.jl:80-112); the window is ordered by the first x point of
 //    each stencil (a stable counting sort), and each thread then owns grid
@@ -53,20 +53,6 @@ struct SlabGeom {
 __host__ __device__ constexpr int slab_pitch(int Mx) {
     return ((2 * padded_len(Mx / 2) + 23) / 32) * 32 + 8;
 }
-
-// Spread launch shape per element type and x length. At x length 512 in
-// Float32 the slab's 24 rows take 16 lanes each for their x transform, 12
-// warps in all: a block of 384 threads transforms them in one round, its
-// windows hold 256 entries (one per thread of the set-up; a slab's list
-// usually fits one window) and two blocks fit per SM. Otherwise 256 threads
-// and windows of 128 entries.
-template <typename T, int H>
-struct SpreadShape {
-    static constexpr bool WIDE = sizeof(T) == 4 && H == 256;
-    static constexpr int NT = WIDE ? 384 : 256;
-    static constexpr int CAP = WIDE ? 256 : SLAB_CAP;
-    static constexpr int MINB = WIDE ? 2 : (sizeof(T) == 4 ? 3 : 2);
-};
 
 // Slab shape per element type and x length (3*BY*BZ rows in shared memory).
 template <typename T, int H>
@@ -245,16 +231,14 @@ __global__ void k_slab_lists(const vec4<T>* __restrict__ Ys, const int32_t* __re
 template <typename T, int BY, int BZ, int H>
 struct SpreadWin {
     static constexpr int NRP = BY * BZ;
-    static constexpr int CAP = SpreadShape<T, H>::CAP;
-    static_assert(CAP <= 256, "entry indices are packed in 8 bits of the sort keys");
-    int key[CAP];        // first x point of the stencil, in [0, Mx)
-    unsigned msk[CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15) | first x + 32768 (16..31)
-    T y0[CAP];
-    T f[3][CAP];
+    int key[SLAB_CAP];        // first x point of the stencil, in [0, Mx)
+    unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15) | first x + 32768 (16..31)
+    T y0[SLAB_CAP];
+    T f[3][SLAB_CAP];
     // rows padded by one element: lanes reading different entries at the same
     // slab row then fall into different banks
-    T gyz[CAP][NRP + 1], dyz[CAP][NRP + 1];   // gy gz and gy gz (r2y + r2z)
-    unsigned sk[CAP];    // sort keys (key << 8 | entry), in sorted order
+    T gyz[SLAB_CAP][NRP + 1], dyz[SLAB_CAP][NRP + 1];   // gy gz and gy gz (r2y + r2z)
+    unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry), in sorted order
     int first[2 * H + 1];     // counting-sort bins: entries with key <= v
     int scan[32];
 };
@@ -375,7 +359,7 @@ __device__ __forceinline__ void slab_x_r2c(T* acc, cplx<T>* __restrict__ spec, i
 
 // ---- spread into a slab, then x-r2c straight into the spectrum -----------
 template <typename T, int H, int BY, int BZ>
-__global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB) k_spread_slab(const vec4<T>* __restrict__ Ys,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(const vec4<T>* __restrict__ Ys,
                                                      const vec4<T>* __restrict__ Fs,
                                                      const int32_t* __restrict__ off,
                                                      cplx<T>* __restrict__ spec, int hxp,
@@ -384,7 +368,6 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
                                                      const int* __restrict__ lists,
                                                      const int* __restrict__ counts) {
     constexpr int Mx = 2 * H, P = slab_pitch(Mx), NRP = BY * BZ, ROWS = 3 * NRP;
-    constexpr int CAP = SpreadShape<T, H>::CAP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T* acc = reinterpret_cast<T*>(smem_raw);
     SpreadWin<T, BY, BZ, H>& W = *reinterpret_cast<SpreadWin<T, BY, BZ, H>*>(acc + ROWS * P);
@@ -411,8 +394,7 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
         if ((int)threadIdx.x < count) atomicAdd(&fe[W.key[threadIdx.x]], 1);
         __syncthreads();
         {
-            constexpr int NT = SpreadShape<T, H>::NT;
-            constexpr int BPT = (Mx + NT - 1) / NT;   // bins per thread
+            constexpr int BPT = (Mx + 255) / 256;   // bins per thread (256 threads)
             int cnt[BPT], sum = 0;
 #pragma unroll
             for (int u = 0; u < BPT; ++u) {
@@ -441,7 +423,7 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
                 const int pos = act ? fe[key] + below : 0;
                 __syncwarp();
                 if (act && below == __popc(grp) - 1) fe[key] += __popc(grp);
-                if (act) W.sk[pos] = ((unsigned)key << 8) | (unsigned)i;
+                if (act) W.sk[pos] = ((unsigned)key << 7) | (unsigned)i;
                 __syncwarp();
             }
         }
@@ -467,8 +449,8 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
                 }
                 for (int kk = kb; kk < ke; ++kk) {
                     const unsigned v = W.sk[kk];
-                    const int i = (int)(v & 255u);
-                    int e = x - (int)(v >> 8);
+                    const int i = (int)(v & 127u);
+                    int e = x - (int)(v >> 7);
                     if (e < 0) e += Mx;
                     const T y0 = W.y0[i];
                     const unsigned m = W.msk[i];
@@ -508,8 +490,8 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
     const int stored = counts[cta];
     if (stored >= 0) {
         const int* glist = lists + (int64_t)cta * g.lcap;
-        for (int w0 = 0; w0 < stored; w0 += CAP) {
-            const int n = min(CAP, stored - w0);
+        for (int w0 = 0; w0 < stored; w0 += SLAB_CAP) {
+            const int n = min(SLAB_CAP, stored - w0);
             if ((int)threadIdx.x < n) {
                 const int s = glist[w0 + threadIdx.x];
                 const vec4<T> y = Ys[s];
@@ -523,25 +505,25 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
             __syncthreads();
         }
     } else {
-        // the list overflowed: scan the candidates in chunks of CAP and
+        // the list overflowed: scan the candidates in chunks of SLAB_CAP and
         // compact the touching ones into windows, in candidate order
         const SlabRows rows = slab_rows<BY, BZ>(g, y0r, z0r);
         int count = 0;
         for (int pi = 0; pi < rows.ny * rows.nz; ++pi) {
             const int c0 = slab_row_cell(g, rows, pi);
             const int sb = off[c0], se = off[c0 + g.m0];
-            for (int b = sb; b < se; b += CAP) {
+            for (int b = sb; b < se; b += SLAB_CAP) {
                 const int s = b + (int)threadIdx.x;
                 unsigned m = 0;
                 int sx = 0, sy = 0, sz = 0;
                 vec4<T> y{};
-                if ((int)threadIdx.x < CAP && s < se) {
+                if ((int)threadIdx.x < SLAB_CAP && s < se) {
                     y = Ys[s];
                     slab_anchor<T, BY, BZ>(p, y, y0r, z0r, sx, sy, sz, m);
                 }
                 int tot;
                 const int pre = block_scan(m ? 1 : 0, W.scan, tot);
-                if (count + tot > CAP) {   // block-uniform
+                if (count + tot > SLAB_CAP) {   // block-uniform
                     process(count);
                     __syncthreads();
                     count = 0;
@@ -572,7 +554,7 @@ __host__ __device__ constexpr unsigned slab_row_copy_bytes() {
 }
 
 template <typename T, int H, int BY, int BZ>
-__global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB) k_interp_slab(const vec4<T>* __restrict__ Ys,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(const vec4<T>* __restrict__ Ys,
                                                      const int32_t* __restrict__ off,
                                                      const cplx<T>* __restrict__ spec, int hxp,
                                                      T* __restrict__ Vs, StencilParams<T> p,
@@ -585,12 +567,11 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
     static_assert((P * sizeof(T)) % 16 == 0, "slab rows must start on 16-byte boundaries");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar[2];
-    // rows of the first transform round of the 16 x L path (NT / L); when
+    // rows of the first transform round of the 16 x L path (256 / L); when
     // they are fewer than the slab's, the rest arrive on a second barrier and
-    // land while the first round runs (the block shape is the spread's)
-    constexpr int NT = SpreadShape<T, H>::NT;
+    // land while the first round runs
     constexpr bool R16 = sizeof(T) == 4 && (H == 64 || H == 128 || H == 256);
-    constexpr int R1 = R16 && NT / (H / 16) < ROWS ? NT / (H / 16) : ROWS;
+    constexpr int R1 = R16 && 256 / (H / 16) < ROWS ? 256 / (H / 16) : ROWS;
     T* acc = reinterpret_cast<T*>(smem_raw);
     cplx<T>* dummy = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
     cplx<T>* tw = dummy + padded_len(H);   // FFT twiddles in shared memory
@@ -631,7 +612,7 @@ __global__ void __launch_bounds__(SpreadShape<T, H>::NT, SpreadShape<T, H>::MINB
         constexpr int L = H / 16;
         static_assert(ROWS % (32 / L) == 0, "a warp's rows must be all present or all absent");
         static_assert(2 * 16 * (L + 1) <= P, "the exchange scratch must fit a slab row");
-        static_assert(R1 == ROWS || R1 == NT / L, "the first round covers NT / L rows");
+        static_assert(R1 == ROWS || R1 == 256 / L, "the first round covers 256 / L rows");
         const int t = threadIdx.x & (L - 1);
         for (int r0 = 0; r0 < ROWS; r0 += R1) {
             if (r0 > 0 && !landed(1)) return;   // block-uniform
@@ -763,7 +744,6 @@ using InterpSlabKernel = void (*)(const vec4<T>*, const int32_t*, const cplx<T>*
 template <typename T>
 struct SlabKernels {
     SpreadSlabKernel<T> spread_fused = nullptr;
-    int spread_threads = 256;
     InterpSlabKernel<T> interp = nullptr;
     ListsKernel<T> lists = nullptr;
     int BY = 0, BZ = 0;
@@ -776,7 +756,6 @@ SlabKernels<T> slab_kernels_for() {
     constexpr int BY = SlabShape<T, H>::BY, BZ = SlabShape<T, H>::BZ;
     SlabKernels<T> k;
     k.spread_fused = k_spread_slab<T, H, BY, BZ>;
-    k.spread_threads = SpreadShape<T, H>::NT;
     k.interp = k_interp_slab<T, H, BY, BZ>;
     k.lists = k_slab_lists<T, BY, BZ>;
     k.BY = BY;

@@ -24,9 +24,12 @@ CASES = {"64^3": dict(L=(40.0,) * 3, N=2000, M=(64, 64, 64)),
          "64x1024x64": dict(L=(40.0, 640.0, 40.0), N=32000, M=(64, 1024, 64)),
          "1024x64x64": dict(L=(640.0, 40.0, 40.0), N=32000, M=(1024, 64, 64)),
          # lines of 512 along y
-         "64x512x64": dict(L=(40.0, 320.0, 40.0), N=16000, M=(64, 512, 64))}
+         "64x512x64": dict(L=(40.0, 320.0, 40.0), N=16000, M=(64, 512, 64)),
+         # lines of 256 and 512 along z (the in-place wide-tile z pass)
+         "64x64x256": dict(L=(40.0, 40.0, 160.0), N=8000, M=(64, 64, 256)),
+         "64x64x512": dict(L=(40.0, 40.0, 320.0), N=16000, M=(64, 64, 512))}
 Y_VARIANTS = [(k, B) for k in (0, 1, 2) for B in (2, 4, 8, 16)]
-Z_VARIANTS = [(k, B) for k in (0, 1, 2, 3) for B in (2, 4, 8, 16)]
+Z_VARIANTS = [(k, B) for k in (0, 1, 2, 3, 4) for B in (2, 4, 8, 16)]
 
 
 def _solve(ffcm, T, case, env):
