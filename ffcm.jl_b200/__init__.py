@@ -37,7 +37,8 @@ __all__ = ["FFCMConfig", "mobility", "FFCMMobility", "FFCMBatch", "ArgumentError
            "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities",
            "mobility_checkpoint", "adjoint", "objective_gradient", "rrule_mobility",
            "mobility_autograd", "cg", "CGHistory", "wisdom_export", "wisdom_import", "batch_offsets",
-           "pack_batch", "unpack_batch"]
+           "pack_batch", "unpack_batch", "dist_partition", "DistributedConfig", "TorchExchange",
+           "distributed_mobility_local"]
 
 
 class ArgumentError(ValueError):
@@ -889,3 +890,160 @@ class FFCMBatch:
         st = _stream_of(v) if stream is None else _stream_handle(stream)
         _raise(L_.load().ffcm_batch_mobility(self._b, v.ptr, y.ptr, f.ptr, v.memory, st))
         return V
+
+
+# ---- one system over several GPUs: z-slab decomposition (ffcm_dist_*) ----
+
+def dist_partition(T, num_grid_points, nranks, rank):
+    """``(z_begin, z_end, kx_begin, kx_end)`` of ``rank`` in a z-slab
+    decomposition over ``nranks`` (host only: ``ffcm_dist_partition``)."""
+    out = (ctypes.c_int32 * 4)()
+    _raise(L_.load().ffcm_dist_partition(_dtype_code(T), _i32ptr(num_grid_points), int(nranks), int(rank), out))
+    return tuple(int(v) for v in out)
+
+
+class _DeviceArray:
+    """A device buffer of the library seen by torch without a copy
+    (``__cuda_array_interface__``)."""
+
+    def __init__(self, ptr, count, typestr, device):
+        self.__cuda_array_interface__ = {"shape": (int(count),), "typestr": typestr,
+                                         "data": (int(ptr), False), "version": 3}
+        self.device = device
+
+    def tensor(self):
+        import torch
+        return torch.as_tensor(self, device=f"cuda:{self.device}")
+
+
+class TorchExchange:
+    """The collectives of a z-slab decomposition through torch.distributed:
+    the two spectrum transposes as ``all_to_all_single`` of R equal blocks and
+    the interpolation shares as an ``all_reduce`` (sum). With the NCCL backend
+    the tensors stay on the GPU."""
+
+    def __init__(self, group=None):
+        self.group = group
+
+    def all_to_all(self, recv, send):
+        import torch.distributed as dist
+        dist.all_to_all_single(recv, send, group=self.group)
+
+    def all_reduce(self, partial):
+        import torch.distributed as dist
+        dist.all_reduce(partial, op=dist.ReduceOp.SUM, group=self.group)
+
+
+class DistributedConfig:
+    """One rank of a configuration split over ``nranks`` GPUs by z slabs
+    (``ffcm_dist_create``): the same parameters as ``FFCMConfig``, the grid
+    divided so that each GPU holds 1 / nranks of the spectrum. The particles
+    are replicated. ``mobility(V, Y, F, exchange)`` runs the steps of
+    ``ffcm_dist_*`` with the exchange's collectives between them; every rank
+    receives all N velocities. No reference counterpart (the reference solves
+    one system per device)."""
+
+    def __init__(self, T=np.float32, *, rank, nranks, L, R_c, N, a=1.0, kernel_widths_ratio, num_grid_points,
+                 M_G, viscosity, device=0, stencil=None, **_ignored):
+        self._h = None
+        self.T = np.dtype(T).type
+        self.rank, self.nranks, self.device, self.N = int(rank), int(nranks), int(device), int(N)
+        lib = L_.load()
+        h = ctypes.c_void_p()
+        _raise(lib.ffcm_dist_create(ctypes.byref(h), _dtype_code(T), _dptr(L), float(R_c), int(N), float(a),
+                                    float(kernel_widths_ratio), _i32ptr(num_grid_points), int(M_G),
+                                    float(viscosity), int(nranks), int(rank), int(device)))
+        self._h = h
+        if stencil is not None:
+            _raise(lib.ffcm_set_stencil(h, L_.STENCIL[stencil]))
+        send, recv, part = ctypes.c_void_p(), ctypes.c_void_p(), ctypes.c_void_p()
+        blk = ctypes.c_int64()
+        rng = (ctypes.c_int32 * 4)()
+        _raise(lib.ffcm_dist_buffers(h, ctypes.byref(send), ctypes.byref(recv), ctypes.byref(blk),
+                                     ctypes.byref(part), rng))
+        self.ranges = tuple(int(v) for v in rng)
+        tstr = "<f4" if self.T == np.float32 else "<f8"
+        words = int(blk.value) // np.dtype(self.T).itemsize * int(nranks)
+        self.send = _DeviceArray(send.value, words, tstr, self.device).tensor()
+        self.recv = _DeviceArray(recv.value, words, tstr, self.device).tensor()
+        self.partial = _DeviceArray(part.value, 3 * self.N, tstr, self.device).tensor()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L_.load().ffcm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # the steps, on the current torch stream
+    def _stream(self):
+        import torch
+        return _stream_handle(torch.cuda.current_stream(self.device))
+
+    def forward(self, Y, F):
+        y, f = _particle_args(self, (("Y", Y), ("F", F)))
+        _raise(L_.load().ffcm_dist_forward(self._h, y.ptr, f.ptr, y.memory,
+                                           self._stream() if y.memory == L_.DEVICE else None))
+
+    def stokes(self):
+        _raise(L_.load().ffcm_dist_stokes(self._h, self._stream()))
+
+    def interpolate(self):
+        _raise(L_.load().ffcm_dist_interpolate(self._h, self._stream()))
+
+    def correct(self, V):
+        (v,) = _particle_args(self, (("V", V),), writable=("V",))
+        _raise(L_.load().ffcm_dist_correct(self._h, v.ptr, v.memory,
+                                           self._stream() if v.memory == L_.DEVICE else None))
+        return V
+
+    def mobility(self, V, Y, F, exchange):
+        """V = M(Y) F for the whole system, this rank's share of the work and
+        the exchange's collectives in between."""
+        self.forward(Y, F)
+        exchange.all_to_all(self.recv, self.send)
+        self.stokes()
+        exchange.all_to_all(self.recv, self.send)
+        self.interpolate()
+        exchange.all_reduce(self.partial)
+        return self.correct(V)
+
+
+def distributed_mobility_local(configs, Vs, Y, F):
+    """All ranks of a decomposition driven from one process (one GPU or
+    several): the collectives become copies between the ranks' buffers, in
+    the order the processes of a real run would perform them. ``Vs`` holds
+    one output array per rank."""
+    import torch
+    R = len(configs)
+    for c in configs:
+        c.forward(Y, F)
+
+    def exchange():
+        blocks = [c.send.view(R, -1).clone() for c in configs]
+        for r, c in enumerate(configs):
+            for q in range(R):
+                c.recv.view(R, -1)[q].copy_(blocks[q][r])
+
+    for c in configs:
+        torch.cuda.current_stream(c.device).synchronize()
+    exchange()
+    for c in configs:
+        c.stokes()
+    for c in configs:
+        torch.cuda.current_stream(c.device).synchronize()
+    exchange()
+    for c in configs:
+        c.interpolate()
+    for c in configs:
+        torch.cuda.current_stream(c.device).synchronize()
+    total = sum(c.partial.clone() for c in configs)
+    for c in configs:
+        c.partial.copy_(total)
+    for c, V in zip(configs, Vs):
+        c.correct(V)
+    return Vs

@@ -99,6 +99,14 @@ SIGNATURES = {
     "ffcm_mobility_apply": (_c.c_int, [_vp, _vp, _vp, _i32, _vp]),
     "ffcm_cg_solve": (_c.c_int, [_vp, _vp, _vp, _i32, _c.c_double, _c.c_double, _i32, _i32, _vp, _vp, _vp,
                                  _vp]),
+    "ffcm_dist_partition": (_c.c_int, [_i32, _i32p, _i32, _i32, _i32p]),
+    "ffcm_dist_create": (_c.c_int, [_c.POINTER(_vp), _i32, _dp, _d, _i64, _d, _d, _i32p, _i32, _d, _i32, _i32,
+                                    _i32]),
+    "ffcm_dist_buffers": (_c.c_int, [_vp, _c.POINTER(_vp), _c.POINTER(_vp), _i64p, _c.POINTER(_vp), _i32p]),
+    "ffcm_dist_forward": (_c.c_int, [_vp, _vp, _vp, _i32, _vp]),
+    "ffcm_dist_stokes": (_c.c_int, [_vp, _vp]),
+    "ffcm_dist_interpolate": (_c.c_int, [_vp, _vp]),
+    "ffcm_dist_correct": (_c.c_int, [_vp, _vp, _i32, _vp]),
 }
 
 _lib = None

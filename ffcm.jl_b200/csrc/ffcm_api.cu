@@ -284,6 +284,12 @@ struct EngineBase {
                          double abstol, int maxiter, cudaStream_t s) = 0;
     virtual int cg_iteration(void* x, void* r, void* p, void* q, CgState* st, cudaGraphConditionalHandle loop,
                              cudaStream_t s) = 0;
+    // a rank of a z-slab decomposition (see ffcm_dist_*)
+    virtual int dist_forward(const void* Y, const void* F, cudaStream_t s) = 0;
+    virtual int dist_stokes(cudaStream_t s) = 0;
+    virtual int dist_interp(cudaStream_t s) = 0;
+    virtual int dist_correct(void* V, cudaStream_t s) = 0;
+    virtual void dist_info(void** send, void** recv, int64_t* block_bytes, void** partial, int32_t* ranges) const = 0;
 };
 
 }  // namespace
@@ -295,6 +301,9 @@ struct ffcm_handle {
     int32_t M[3] = {0, 0, 0};
     int32_t M_G = 0;
     int32_t stencil = FFCM_STENCIL_REFERENCE;   // stencil arithmetic (FFCM_STENCIL_*)
+    // a rank of a z-slab decomposition of one system (ffcm_dist_create)
+    bool distributed = false;
+    int32_t nranks = 1, rank = 0;
     int32_t num_cells[3] = {0, 0, 0};
     int64_t ncell = 0;
     size_t esize = 4;
@@ -376,6 +385,36 @@ int grid_for(int64_t n, int threads, int cap = 148 * 16) {
     return (int)std::min<int64_t>(b, cap);
 }
 
+// ---------------------------------------------------------------------------
+// z-slab decomposition of one system over R ranks: rank r holds the z planes
+// [zb, ze) (whole slabs of BZ planes) for the spread, the y passes and the
+// interpolation, and the kx columns [kb, ke) of every plane for the z pass.
+// Contiguous ranges, as even as possible.
+void dist_ranges(int Mz, int BZ, int nkx, int R, int r, int& zb, int& ze, int& kb, int& ke) {
+    const int nzs = Mz / BZ;
+    zb = (int)((int64_t)nzs * r / R) * BZ;
+    ze = (int)((int64_t)nzs * (r + 1) / R) * BZ;
+    kb = (int)((int64_t)nkx * r / R);
+    ke = (int)((int64_t)nkx * (r + 1) / R);
+}
+
+// dst[c dc + z dz + y dy + k] = src[c sc + z sz + y sy + k] for c < 3, z < nz,
+// y < ny, k < nk: one block of a spectrum transpose (a row of k per thread
+// group, coalesced on both sides).
+template <typename T>
+__global__ void k_copy_block(cplx<T>* __restrict__ dst, int64_t dc, int64_t dz, int64_t dy,
+                             const cplx<T>* __restrict__ src, int64_t sc, int64_t sz, int64_t sy, int nz, int ny,
+                             int nk) {
+    const int rows = 3 * nz * ny;
+    for (int row = blockIdx.x; row < rows; row += gridDim.x) {
+        const int y = row % ny, t = row / ny;
+        const int z = t % nz, c = t / nz;
+        cplx<T>* d = dst + c * dc + z * dz + y * dy;
+        const cplx<T>* s = src + c * sc + z * sz + y * sy;
+        for (int k = threadIdx.x; k < nk; k += blockDim.x) d[k] = s[k];
+    }
+}
+
 template <typename T>
 struct Engine final : EngineBase {
     ffcm_handle* h;
@@ -408,6 +447,23 @@ struct Engine final : EngineBase {
     bool ymap_ok[5] = {false, false, false, false, false};
     int num_sms = 148;
     size_t smem_fx = 0, smem_fy = 0, smem_fz = 0;
+    // spectrum held: planes (c, z) for z in the mzl planes of `spec` (all Mz
+    // on one GPU, the rank's own z planes in a z-slab decomposition); the z
+    // pass works on zbuf: nkz columns (global columns kzoff ...) of pitch
+    // zpitch over all Mz planes (on one GPU zbuf = spec)
+    int mzl = 0;
+    cplx<T>* zbuf = nullptr;
+    int zpitch = 0, nkz = 0, kzoff = 0;
+    // z-slab decomposition (nranks > 1 or an explicitly distributed handle)
+    struct Dist {
+        bool on = false;
+        int R = 1, r = 0;
+        std::vector<int> zb, ze, kb, ke;   // per rank: z planes [zb, ze), kx columns [kb, ke)
+        int mzl_max = 0, nk_max = 0;
+        int64_t blk = 0;                   // complex values per peer block of a transpose
+        cplx<T>* send = nullptr;
+        cplx<T>* recv = nullptr;
+    } dist;
     // slab kernels: spread/interpolation fused with the x transforms
     bool slab = false;
     SlabKernels<T> sk;
@@ -568,12 +624,25 @@ struct Engine final : EngineBase {
             sg.h = (double)d.h;
             sg.nty = My / sk.BY;
             sg.ntz = Mz / sk.BZ;
+            sg.zs0 = 0;
+            sg.mz_loc = Mz;
             // expected touching particles per slab: N x (rows reached)/(rows total)
             const double expect = (double)N * (sk.BY + MG - 1) * (sk.BZ + MG - 1) / ((double)My * Mz);
             sg.lcap = (int)std::min<double>(1 << 20, std::max(256.0, 4.0 * expect + 64.0));
             sg.lcap = (sg.lcap + 31) / 32 * 32;
             TRY(raise_smem_cap((const void*)sk.spread_fused, sk.smem));
             TRY(raise_smem_cap((const void*)sk.interp, sk.smem_interp));
+        }
+        mzl = Mz;
+        zpitch = hxp;
+        nkz = nkx;
+        kzoff = 0;
+        if (h->distributed) {
+            if (!(slab && fast_x && fast_y && fast_z))
+                return fail(FFCM_ERR_UNSUPPORTED,
+                            "a z-slab decomposition needs the fused slab path: power-of-two grid sides of 64..2048 "
+                            "(x), 32..1024 (y, z) and M_G = 8");
+            TRY(dist_setup(align));
         }
         if (fast_y) {
             int cand[4];
@@ -605,7 +674,7 @@ struct Engine final : EngineBase {
                 TRY(raise_smem_cap((const void*)zin_kernel<T>(Mz, B), zin_smem<T>(Mz, B)));
             if (fast_z && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= budget)
                 TRY(raise_smem_cap((const void*)zlr_kernel<T>(Mz, B), FastFft<T>::zlr_smem(Mz, B)));
-            if (fast_z && zpipe_kernel<T>(Mz, B) && hxp % B == 0 && zpipe_smem<T>(Mz, B) <= budget)
+            if (fast_z && zpipe_kernel<T>(Mz, B) && zpitch % B == 0 && zpipe_smem<T>(Mz, B) <= budget)
                 TRY(raise_smem_cap((const void*)zpipe_kernel<T>(Mz, B), zpipe_smem<T>(Mz, B)));
         }
         TRY(raise_smem_cap((const void*)k_fft_x_r2c<T>, smem_x));
@@ -632,7 +701,17 @@ struct Engine final : EngineBase {
         TRY(alloc(scratch_i, std::max<size_t>(N, (size_t)ncell + 1)));
         TRY(alloc(Ys, N));
         TRY(alloc(Fs, N));
-        TRY(alloc(spec, 3 * (size_t)hxp * My * Mz));
+        TRY(alloc(spec, 3 * (size_t)hxp * My * mzl));
+        if (dist.on) {
+            TRY(alloc(zbuf, 3 * (size_t)zpitch * My * Mz));
+            TRY(alloc(dist.send, (size_t)dist.R * dist.blk));
+            TRY(alloc(dist.recv, (size_t)dist.R * dist.blk));
+            CUDA_TRY(cudaMemset(zbuf, 0, 3 * (size_t)zpitch * My * Mz * sizeof(cplx<T>)));
+            CUDA_TRY(cudaMemset(dist.send, 0, (size_t)dist.R * dist.blk * sizeof(cplx<T>)));
+            CUDA_TRY(cudaMemset(dist.recv, 0, (size_t)dist.R * dist.blk * sizeof(cplx<T>)));
+        } else {
+            zbuf = spec;
+        }
         TRY(alloc(twx, Mx));
         TRY(alloc(twy, My));
         TRY(alloc(twz, Mz));
@@ -646,7 +725,7 @@ struct Engine final : EngineBase {
         }
 
         // zero-initialised grids and cell list (src/config.jl:443-448)
-        CUDA_TRY(cudaMemset(spec, 0, 3 * (size_t)hxp * My * Mz * sizeof(cplx<T>)));
+        CUDA_TRY(cudaMemset(spec, 0, 3 * (size_t)hxp * My * mzl * sizeof(cplx<T>)));
         if (fast_z || fast_y) make_tma_maps();
         CUDA_TRY(cudaMemset(off, 0, ((size_t)ncell + 1) * sizeof(int32_t)));
         CUDA_TRY(cudaMemset(perm, 0, (size_t)N * sizeof(int32_t)));
@@ -718,31 +797,32 @@ struct Engine final : EngineBase {
         return FFCM_OK;
     }
 
-    // Spectrum as a 3-D tensor (kx, y, c * Mz + z) of 8-byte words, boxes of
-    // B kx columns x 1 y x min(256, Mz) rows.
-    // Spectrum as a 3-D tensor (kx, y, c * Mz + z) of 8-byte words. z pass:
-    // boxes of B kx columns x 1 y x min(256, Mz) rows; y pass: B kx columns x
-    // min(256, My) rows x 1 plane.
+    // The spectrum as 3-D tensors of 8-byte words for the tiled bulk copies:
+    // y pass: `spec` as (kx, y, c mzl + z), boxes of B kx columns x
+    // min(256, My) rows x 1 plane; z pass: `zbuf` as (kx, y, c Mz + z), boxes
+    // of B kx columns x 1 y x min(256, Mz) rows (the component and z axes merge
+    // because a component's stride is the plane count times the z stride).
     void make_tma_maps() {
         TensorMapEncodeFn enc = tensor_map_encoder();
         if (!enc) return;
         constexpr int EPC = TmaElem<T>::PER_CPLX;
-        const cuuint64_t dims[3] = {(cuuint64_t)hxp * EPC, (cuuint64_t)My, (cuuint64_t)3 * Mz};
-        const cuuint64_t strides[2] = {(cuuint64_t)hxp * sizeof(cplx<T>), (cuuint64_t)My * hxp * sizeof(cplx<T>)};
         const cuuint32_t estr[3] = {1, 1, 1};
         const CUtensorMapDataType dt = sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_UINT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-        auto make = [&](CUtensorMap* m, cuuint32_t bx, cuuint32_t by, cuuint32_t bz) {
+        auto make = [&](CUtensorMap* m, void* base, int pitch, int planes, cuuint32_t bx, cuuint32_t by,
+                        cuuint32_t bz) {
+            const cuuint64_t dims[3] = {(cuuint64_t)pitch * EPC, (cuuint64_t)My, (cuuint64_t)planes};
+            const cuuint64_t strides[2] = {(cuuint64_t)pitch * sizeof(cplx<T>),
+                                           (cuuint64_t)My * pitch * sizeof(cplx<T>)};
             const cuuint32_t box[3] = {bx, by, bz};
-            return enc(m, dt, 3, spec, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            return enc(m, dt, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                        CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
         };
         for (int i = 1, B = 2; B <= 16; ++i, B *= 2) {
-            if (hxp % B != 0) continue;
-            if (fast_z && (ztma_kernel<T>(Mz, B) || zin_kernel<T>(Mz, B)))
-                zmap_ok[i] = make(&zmap[i], (cuuint32_t)(B * EPC), 1, (cuuint32_t)tma_zbox(Mz));
-            if (fast_y && ytma_kernel<T>(My, B))
-                ymap_ok[i] = make(&ymap[i], (cuuint32_t)(B * EPC), (cuuint32_t)tma_zbox(My), 1);
+            if (fast_z && zpitch % B == 0 && (ztma_kernel<T>(Mz, B) || zin_kernel<T>(Mz, B)))
+                zmap_ok[i] = make(&zmap[i], zbuf, zpitch, 3 * Mz, (cuuint32_t)(B * EPC), 1, (cuuint32_t)tma_zbox(Mz));
+            if (fast_y && hxp % B == 0 && ytma_kernel<T>(My, B))
+                ymap_ok[i] = make(&ymap[i], spec, hxp, 3 * mzl, (cuuint32_t)(B * EPC), (cuuint32_t)tma_zbox(My), 1);
         }
     }
 
@@ -779,7 +859,7 @@ struct Engine final : EngineBase {
         if (fast_z) {
             const int k = t.zkind, B = t.Bz;
             const bool ok = (k == 0 && z_kernel<T>(Mz, B) && in_bundles(Mz, B, z_bundles)) ||
-                            (k == 1 && zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
+                            (k == 1 && zpipe_kernel<T>(Mz, B) && zpitch % B == 0 &&
                              zpipe_smem<T>(Mz, B) <= 200 * 1024 && t.zgrid >= 1) ||
                             (k == 2 && zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= 200 * 1024) ||
                             (k == 3 && ztma_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
@@ -811,7 +891,9 @@ struct Engine final : EngineBase {
         int fyk, fyB, fzk, fzB;
         forced_variant("FFCM_FORCE_Y", fyk, fyB);
         forced_variant("FFCM_FORCE_Z", fzk, fzB);
-        const bool forced = fyk >= 0 || fzk >= 0 || std::getenv("FFCM_FORCE_CHUNK") != nullptr;
+        // a rank of a decomposition holds other shapes than its key names: it
+        // neither reuses nor stores choices
+        const bool forced = fyk >= 0 || fzk >= 0 || std::getenv("FFCM_FORCE_CHUNK") != nullptr || dist.on;
         int dev = 0;
         CUDA_TRY(cudaGetDevice(&dev));
         const TuneKey key{dev, (int)sizeof(T), Mx, My, Mz, num_sms};
@@ -850,12 +932,12 @@ struct Engine final : EngineBase {
                     ykind = kind;
                     By = B;
                     if (kind == 1) {
-                        const int ntiles = ((nkx + B - 1) / B) * Mz * 3;
+                        const int ntiles = ((nkx + B - 1) / B) * mzl * 3;
                         TRY(persistent_grid((const void*)ypipe_kernel<T>(My, B), B * (My / 8),
                                             ypipe_smem<T>(My, B), ntiles, ygrid));
                     }
                     if (kind == 2) {
-                        const int ntiles = ((nkx + B - 1) / B) * Mz * 3;
+                        const int ntiles = ((nkx + B - 1) / B) * mzl * 3;
                         TRY(persistent_grid((const void*)ytma_kernel<T>(My, B), B * (My / 8),
                                             ytma_smem<T>(My, B), ntiles, ygrid));
                     }
@@ -876,7 +958,7 @@ struct Engine final : EngineBase {
                     if (kind == 4 && !(zin_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
                                        zin_smem<T>(Mz, B) <= 226 * 1024)) continue;
                     if (kind == 0 && !z_kernel<T>(Mz, B)) continue;
-                    if (kind == 1 && !(zpipe_kernel<T>(Mz, B) && hxp % B == 0 &&
+                    if (kind == 1 && !(zpipe_kernel<T>(Mz, B) && zpitch % B == 0 &&
                                        zpipe_smem<T>(Mz, B) <= 200 * 1024)) continue;
                     if (kind == 2 && !(zlr_kernel<T>(Mz, B) && FastFft<T>::zlr_smem(Mz, B) <= 200 * 1024)) continue;
                     if (kind == 3 && !(ztma_kernel<T>(Mz, B) && zmap_ok[log2i(B)] &&
@@ -891,17 +973,17 @@ struct Engine final : EngineBase {
                     zkind = kind;
                     Bz = B;
                     if (kind == 1) {
-                        const int ntiles = ((nkx + B - 1) / B) * My;
+                        const int ntiles = ((nkz + B - 1) / B) * My;
                         TRY(persistent_grid((const void*)zpipe_kernel<T>(Mz, B), B * (Mz / 8),
                                             zpipe_smem<T>(Mz, B), ntiles, zgrid));
                     }
                     if (kind == 3) {
-                        const int ntiles = ((nkx + B - 1) / B) * My;
+                        const int ntiles = ((nkz + B - 1) / B) * My;
                         TRY(persistent_grid((const void*)ztma_kernel<T>(Mz, B), B * (Mz / 8),
                                             ztma_smem<T>(Mz, B), ntiles, zgrid));
                     }
                     if (kind == 4) {
-                        const int ntiles = ((nkx + B - 1) / B) * My;
+                        const int ntiles = ((nkz + B - 1) / B) * My;
                         TRY(persistent_grid((const void*)zin_kernel<T>(Mz, B), B * (Mz / 8),
                                             zin_smem<T>(Mz, B), ntiles, zgrid));
                     }
@@ -913,7 +995,7 @@ struct Engine final : EngineBase {
             if (fzk >= 0 && best == 1e30f) return fail(FFCM_ERR_ARGUMENT, "FFCM_FORCE_Z names no available z variant");
             zkind = bk; Bz = bB; zgrid = bg;
         }
-        if (fast_y && fast_z) {
+        if (fast_y && fast_z && !dist.on) {
             // chunk widths that keep a chunk's spectrum within ~96 MB of L2
             const double col_bytes = 3.0 * My * Mz * sizeof(cplx<T>);
             float best = 1e30f;
@@ -1110,6 +1192,120 @@ struct Engine final : EngineBase {
                       static_cast<T*>(V), cc, (const T*)partial, h3);
     }
 
+    // ---- z-slab decomposition --------------------------------------------
+    int dist_setup(int align) {
+        dist.on = true;
+        dist.R = h->nranks;
+        dist.r = h->rank;
+        const int nzs = Mz / sk.BZ;
+        if (dist.R < 1 || dist.r < 0 || dist.r >= dist.R)
+            return fail(FFCM_ERR_ARGUMENT, "rank must lie in [0, nranks)");
+        if (dist.R > nzs || dist.R > nkx)
+            return fail(FFCM_ERR_ARGUMENT, "more ranks (" + std::to_string(dist.R) + ") than z slabs (" +
+                                               std::to_string(nzs) + ") or kx columns (" + std::to_string(nkx) + ")");
+        dist.zb.resize(dist.R);
+        dist.ze.resize(dist.R);
+        dist.kb.resize(dist.R);
+        dist.ke.resize(dist.R);
+        for (int q = 0; q < dist.R; ++q) {
+            dist_ranges(Mz, sk.BZ, nkx, dist.R, q, dist.zb[q], dist.ze[q], dist.kb[q], dist.ke[q]);
+            dist.mzl_max = std::max(dist.mzl_max, dist.ze[q] - dist.zb[q]);
+            dist.nk_max = std::max(dist.nk_max, dist.ke[q] - dist.kb[q]);
+        }
+        const int r = dist.r;
+        sg.zs0 = dist.zb[r] / sk.BZ;
+        sg.ntz = (dist.ze[r] - dist.zb[r]) / sk.BZ;
+        sg.mz_loc = dist.ze[r] - dist.zb[r];
+        mzl = sg.mz_loc;
+        kzoff = dist.kb[r];
+        nkz = dist.ke[r] - dist.kb[r];
+        zpitch = ((dist.nk_max + align - 1) / align) * align;
+        dist.blk = 3 * (int64_t)dist.mzl_max * My * dist.nk_max;
+        return FFCM_OK;
+    }
+
+    int copy_block(cplx<T>* dst, int64_t dc, int64_t dz, int64_t dy, const cplx<T>* src, int64_t sc, int64_t sz,
+                   int64_t sy, int nz, int ny, int nk, cudaStream_t s) {
+        if (nz <= 0 || nk <= 0) return FFCM_OK;
+        const int rows = 3 * nz * ny;
+        return launch(h, k_copy_block<T>, std::min(rows, num_sms * 32), 128, 0, s, dst, dc, dz, dy,
+                      (const cplx<T>*)src, sc, sz, sy, nz, ny, nk);
+    }
+
+    // Peer q's block of a transpose buffer: [c][z < mzl_max][y][k < nk_max].
+    int64_t bc() const { return (int64_t)dist.mzl_max * My * dist.nk_max; }
+    int64_t bz() const { return (int64_t)My * dist.nk_max; }
+
+    // Cell list (all particles), own slabs' lists, spread into the own z
+    // planes, y forward; then the first transpose's send blocks: peer q gets
+    // this rank's planes at q's kx columns.
+    int dist_forward(const void* Y, const void* F, cudaStream_t s) override {
+        TRY(wrap_hash(Y, true, true, s));
+        TRY(sort(F, s));
+        TRY(spread_to_spectrum(s, nullptr, true));
+        {
+            StageScope sc(h, FFCM_STAGE_FFT_Y_FWD, s);
+            TRY(launch_y(s, 0));
+        }
+        StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
+        for (int q = 0; q < dist.R; ++q)
+            TRY(copy_block(dist.send + q * dist.blk, bc(), bz(), dist.nk_max, spec + dist.kb[q],
+                           (int64_t)mzl * My * hxp, (int64_t)My * hxp, hxp, mzl, My, dist.ke[q] - dist.kb[q], s));
+        return FFCM_OK;
+    }
+
+    // Received blocks (every rank's planes at this rank's kx columns) into the
+    // z-pass buffer, z pass and projector, and the second transpose's send
+    // blocks: peer q gets its planes at this rank's columns.
+    int dist_stokes(cudaStream_t s) override {
+        StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
+        const int64_t zc = (int64_t)Mz * My * zpitch, zz = (int64_t)My * zpitch;
+        for (int q = 0; q < dist.R; ++q)
+            TRY(copy_block(zbuf + dist.zb[q] * zz, zc, zz, zpitch, dist.recv + q * dist.blk, bc(), bz(), dist.nk_max,
+                           dist.ze[q] - dist.zb[q], My, nkz, s));
+        TRY(launch_z(s));
+        for (int q = 0; q < dist.R; ++q)
+            TRY(copy_block(dist.send + q * dist.blk, bc(), bz(), dist.nk_max, zbuf + dist.zb[q] * zz, zc, zz, zpitch,
+                           dist.ze[q] - dist.zb[q], My, nkz, s));
+        return FFCM_OK;
+    }
+
+    // Received blocks (this rank's planes at every rank's columns) back into
+    // the spectrum, y inverse, and the own slabs' interpolation shares in
+    // `partial` (3N, zeroed first; the host sums it over ranks).
+    int dist_interp(cudaStream_t s) override {
+        {
+            StageScope sc(h, FFCM_STAGE_FFT_Y_INV, s);
+            for (int q = 0; q < dist.R; ++q)
+                TRY(copy_block(spec + dist.kb[q], (int64_t)mzl * My * hxp, (int64_t)My * hxp, hxp,
+                               dist.recv + q * dist.blk, bc(), bz(), dist.nk_max, mzl, My, dist.ke[q] - dist.kb[q], s));
+            TRY(launch_y(s, 1));
+        }
+        return interp_from_spectrum(s);
+    }
+
+    // V = h^3 partial + the pair correction, with `partial` summed over ranks.
+    int dist_correct(void* V, cudaStream_t s) override {
+        StageScope sc(h, FFCM_STAGE_CORRECT, s);
+        return launch(h, corr_tpp(N) == 4 ? k_correct<T, 4> : k_correct<T, 1>, grid_for((int64_t)N * corr_tpp(N), 128),
+                      128, 0, s, N, (const vec4<T>*)Ys, (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
+                      static_cast<T*>(V), cc, (const T*)partial, h3);
+    }
+
+    void dist_info(void** send, void** recv, int64_t* block_bytes, void** partial_out,
+                   int32_t* ranges) const override {
+        if (send) *send = dist.send;
+        if (recv) *recv = dist.recv;
+        if (block_bytes) *block_bytes = dist.blk * (int64_t)sizeof(cplx<T>);
+        if (partial_out) *partial_out = partial;
+        if (ranges) {
+            ranges[0] = dist.zb[dist.r];
+            ranges[1] = dist.ze[dist.r];
+            ranges[2] = dist.kb[dist.r];
+            ranges[3] = dist.ke[dist.r];
+        }
+    }
+
     int spread(cudaStream_t s) override { return spread_from((const vec4<T>*)Fs, s); }
 
     // step API (spread_forces!): depends on Y_sorted/F_sorted only, as the
@@ -1194,60 +1390,61 @@ struct Engine final : EngineBase {
     int launch_y(cudaStream_t s, int inverse, int k0 = 0, int k1 = 0) {
         if (k1 <= 0) k1 = nkx;
         if (fast_y && ykind == 2) {
-            const int ntiles = ((k1 - k0 + By - 1) / By) * Mz * 3;
+            const int ntiles = ((k1 - k0 + By - 1) / By) * mzl * 3;
             return launch(h, ytma_kernel<T>(My, By), std::min(ygrid, ntiles), By * (My / 8), ytma_smem<T>(My, By),
-                          s, ymap[log2i(By)], spec, k0, k1, Mz, hxp, (const cplx<T>*)twy, inverse, h->d_err);
+                          s, ymap[log2i(By)], spec, k0, k1, mzl, hxp, (const cplx<T>*)twy, inverse, h->d_err);
         }
         if (fast_y && ykind == 1) {
-            const int ntiles = ((k1 - k0 + By - 1) / By) * Mz * 3;
+            const int ntiles = ((k1 - k0 + By - 1) / By) * mzl * 3;
             return launch(h, ypipe_kernel<T>(My, By), std::min(ygrid, ntiles), By * (My / 8), ypipe_smem<T>(My, By),
-                          s, spec, k0, k1, Mz, hxp, (const cplx<T>*)twy, inverse);
+                          s, spec, k0, k1, mzl, hxp, (const cplx<T>*)twy, inverse);
         }
         if (fast_y) {
-            dim3 g((k1 - k0 + By - 1) / By, Mz, 3);
+            dim3 g((k1 - k0 + By - 1) / By, mzl, 3);
             return launch(h, y_kernel<T>(My, By), g, By * (My / 8), FastFft<T>::yz_smem(My, By), s, spec,
-                          k0, k1, My, Mz, hxp, (const cplx<T>*)twy, inverse);
+                          k0, k1, My, mzl, hxp, (const cplx<T>*)twy, inverse);
         }
-        dim3 gy((nkx + tx_y - 1) / tx_y, Mz, 3);
-        return launch(h, k_fft_y<T>, gy, 256, smem_y, s, spec, nkx, My, Mz, hxp, plan_y,
+        dim3 gy((nkx + tx_y - 1) / tx_y, mzl, 3);
+        return launch(h, k_fft_y<T>, gy, 256, smem_y, s, spec, nkx, My, mzl, hxp, plan_y,
                       (const cplx<T>*)twy, tx_y, inverse);
     }
 
     int launch_z(cudaStream_t s, int k0 = 0, int k1 = 0) {
-        if (k1 <= 0) k1 = nkx;
+        if (k1 <= 0) k1 = nkz;
+        const T* kxz = kxv + kzoff;   // wavevectors of the columns zbuf holds
         if (fast_z && zkind == 4) {
             const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
             return launch(h, zin_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), zin_smem<T>(Mz, Bz), s,
-                          zmap[log2i(Bz)], spec, k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv,
+                          zmap[log2i(Bz)], zbuf, k0, k1, My, zpitch, (const cplx<T>*)twz, kxz,
                           (const T*)kyv, (const T*)kzv, inv_mu_M, h->d_err);
         }
         if (fast_z && zkind == 3) {
             const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
             return launch(h, ztma_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), ztma_smem<T>(Mz, Bz), s,
-                          zmap[log2i(Bz)], spec, k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv,
+                          zmap[log2i(Bz)], zbuf, k0, k1, My, zpitch, (const cplx<T>*)twz, kxz,
                           (const T*)kyv, (const T*)kzv, inv_mu_M, h->d_err);
         }
         if (fast_z && zkind == 2) {
             dim3 g((k1 - k0 + Bz - 1) / Bz, My, 1);
-            return launch(h, zlr_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::zlr_smem(Mz, Bz), s, spec,
-                          k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+            return launch(h, zlr_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::zlr_smem(Mz, Bz), s, zbuf,
+                          k0, k1, My, zpitch, (const cplx<T>*)twz, kxz, (const T*)kyv,
                           (const T*)kzv, inv_mu_M);
         }
         if (fast_z && zkind == 1) {
             const int ntiles = ((k1 - k0 + Bz - 1) / Bz) * My;
             return launch(h, zpipe_kernel<T>(Mz, Bz), std::min(zgrid, ntiles), Bz * (Mz / 8), zpipe_smem<T>(Mz, Bz),
-                          s, spec, k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+                          s, zbuf, k0, k1, My, zpitch, (const cplx<T>*)twz, kxz, (const T*)kyv,
                           (const T*)kzv, inv_mu_M);
         }
         if (fast_z) {
             dim3 g((k1 - k0 + Bz - 1) / Bz, My, 1);
-            return launch(h, z_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::yz_smem(Mz, Bz), s, spec,
-                          k0, k1, My, hxp, (const cplx<T>*)twz, (const T*)kxv, (const T*)kyv,
+            return launch(h, z_kernel<T>(Mz, Bz), g, Bz * (Mz / 8), FastFft<T>::yz_smem(Mz, Bz), s, zbuf,
+                          k0, k1, My, zpitch, (const cplx<T>*)twz, kxz, (const T*)kyv,
                           (const T*)kzv, inv_mu_M);
         }
-        dim3 gz((nkx + tx_z - 1) / tx_z, My, 1);
-        return launch(h, k_fft_z_stokes<T>, gz, 256, smem_z, s, spec, nkx, My, Mz, hxp, plan_z,
-                      (const cplx<T>*)twz, tx_z, (const T*)kxv, (const T*)kyv, (const T*)kzv, inv_mu_M);
+        dim3 gz((nkz + tx_z - 1) / tx_z, My, 1);
+        return launch(h, k_fft_z_stokes<T>, gz, 256, smem_z, s, zbuf, nkz, My, Mz, zpitch, plan_z,
+                      (const cplx<T>*)twz, tx_z, kxz, (const T*)kyv, (const T*)kzv, inv_mu_M);
     }
 
     int stokes(cudaStream_t s) override {
@@ -1311,6 +1508,15 @@ __global__ void k_add_i32(int32_t* dst, const int32_t* src, int n, int delta) {
 
 int check_handle(const ffcm_handle* h) {
     if (!h || !h->eng) return fail(FFCM_ERR_STATE, "null or destroyed ffcm handle");
+    return FFCM_OK;
+}
+
+// The whole-system entry points: a rank of a z-slab decomposition holds only
+// its own planes of the spectrum and answers to the ffcm_dist_* calls only.
+int check_whole(const ffcm_handle* h) {
+    TRY(check_handle(h));
+    if (h->distributed)
+        return fail(FFCM_ERR_STATE, "a rank of a z-slab decomposition takes the ffcm_dist_* calls only");
     return FFCM_OK;
 }
 
@@ -1519,9 +1725,11 @@ int ffcm_derive_scalars(int32_t dtype, const double* L, double R_c, double a, do
     return FFCM_OK;
 }
 
-int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, int64_t N,
-                double a, double ratio, const int32_t* M, int32_t M_G, double mu,
-                int32_t planning, int32_t threads, int32_t device) {
+// A configuration on `device`; with `distributed`, rank `rank` of a z-slab
+// decomposition over `nranks`.
+static int create_handle(ffcm_handle** out, int32_t dtype, const double* L, double R_c, int64_t N, double a,
+                         double ratio, const int32_t* M, int32_t M_G, double mu, int32_t planning, int32_t threads,
+                         int32_t device, bool distributed, int32_t nranks, int32_t rank) {
     if (!out) return fail(FFCM_ERR_ARGUMENT, "out must not be NULL");
     *out = nullptr;
     TRY(ffcm_validate_config(dtype, L, R_c, N, a, ratio, M, M_G, mu, planning, threads));
@@ -1538,6 +1746,9 @@ int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, i
     for (int i = 0; i < 3; ++i) h->M[i] = M[i];
     h->M_G = M_G;
     h->esize = dtype == FFCM_FLOAT32 ? 4 : 8;
+    h->distributed = distributed;
+    h->nranks = nranks;
+    h->rank = rank;
     {
         const char* v = std::getenv("FFCM_STENCIL");
         if (v && std::strcmp(v, "float64") == 0) h->stencil = FFCM_STENCIL_FLOAT64;
@@ -1558,6 +1769,111 @@ int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, i
     CUDA_TRY(cudaDeviceSynchronize());
     *out = h.release();
     return FFCM_OK;
+}
+
+int ffcm_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, int64_t N,
+                double a, double ratio, const int32_t* M, int32_t M_G, double mu,
+                int32_t planning, int32_t threads, int32_t device) {
+    return create_handle(out, dtype, L, R_c, N, a, ratio, M, M_G, mu, planning, threads, device, false, 1, 0);
+}
+
+int ffcm_dist_partition(int32_t dtype, const int32_t* M, int32_t nranks, int32_t rank, int32_t* ranges) {
+    g_err.clear();
+    if (!M || !ranges) return fail(FFCM_ERR_ARGUMENT, "M and ranges must not be NULL");
+    if (dtype != FFCM_FLOAT32 && dtype != FFCM_FLOAT64)
+        return fail(FFCM_ERR_ARGUMENT, "dtype must be FFCM_FLOAT32 or FFCM_FLOAT64");
+    if (nranks < 1 || rank < 0 || rank >= nranks) return fail(FFCM_ERR_ARGUMENT, "rank must lie in [0, nranks)");
+    if (M[0] < 2 || (M[0] & (M[0] - 1)) || M[2] < 1)
+        return fail(FFCM_ERR_UNSUPPORTED, "a z-slab decomposition needs a power-of-two x side");
+    int BZ = 0;
+    if (dtype == FFCM_FLOAT32) {
+        SlabKernels<float> k;
+        if (!slab_kernels<float>(M[0] / 2, k)) return fail(FFCM_ERR_UNSUPPORTED, "no slab kernels for this x side");
+        BZ = k.BZ;
+    } else {
+        SlabKernels<double> k;
+        if (!slab_kernels<double>(M[0] / 2, k)) return fail(FFCM_ERR_UNSUPPORTED, "no slab kernels for this x side");
+        BZ = k.BZ;
+    }
+    const int nkx = M[0] / 2 + 1;
+    if (M[2] % BZ != 0 || nranks > M[2] / BZ || nranks > nkx)
+        return fail(FFCM_ERR_ARGUMENT, "more ranks than z slabs or kx columns");
+    dist_ranges(M[2], BZ, nkx, nranks, rank, ranges[0], ranges[1], ranges[2], ranges[3]);
+    return FFCM_OK;
+}
+
+int ffcm_dist_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, int64_t N, double a,
+                     double ratio, const int32_t* M, int32_t M_G, double mu, int32_t nranks, int32_t rank,
+                     int32_t device) {
+    return create_handle(out, dtype, L, R_c, N, a, ratio, M, M_G, mu, FFCM_FFT_ESTIMATE, 1, device, true, nranks,
+                         rank);
+}
+
+int ffcm_dist_buffers(const ffcm_handle* h, void** send, void** recv, int64_t* block_bytes, void** partial,
+                      int32_t* ranges) {
+    g_err.clear();
+    TRY(check_handle(h));
+    if (!h->distributed) return fail(FFCM_ERR_STATE, "not a rank of a z-slab decomposition (ffcm_dist_create)");
+    h->eng->dist_info(send, recv, block_bytes, partial, ranges);
+    return FFCM_OK;
+}
+
+int ffcm_dist_forward(ffcm_handle* h, const void* Y, const void* F, int32_t memory, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    if (!h->distributed) return fail(FFCM_ERR_STATE, "not a rank of a z-slab decomposition (ffcm_dist_create)");
+    TRY(check_args(h->device, memory, {Y, F}));
+    if (!Y || !F) return fail(FFCM_ERR_ARGUMENT, "Y and F must not be NULL");
+    h->ckpt = false;
+    h->positions = false;
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    const size_t bytes = 3 * (size_t)h->N * h->esize;
+    const void *Yd = Y, *Fd = F;
+    if (memory == FFCM_HOST) {
+        StageScope sc(h, FFCM_STAGE_H2D, s);
+        CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));
+        CUDA_TRY(cudaMemcpyAsync(e->F_in(), F, bytes, cudaMemcpyHostToDevice, s));
+        Yd = e->Y_in();
+        Fd = e->F_in();
+    }
+    TRY(e->dist_forward(Yd, Fd, s));
+    return memory == FFCM_HOST ? finish(h, s) : FFCM_OK;
+}
+
+int ffcm_dist_stokes(ffcm_handle* h, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    if (!h->distributed) return fail(FFCM_ERR_STATE, "not a rank of a z-slab decomposition (ffcm_dist_create)");
+    DeviceGuard g(h->device);
+    return h->eng->dist_stokes(h->pick(stream));
+}
+
+int ffcm_dist_interpolate(ffcm_handle* h, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    if (!h->distributed) return fail(FFCM_ERR_STATE, "not a rank of a z-slab decomposition (ffcm_dist_create)");
+    DeviceGuard g(h->device);
+    return h->eng->dist_interp(h->pick(stream));
+}
+
+int ffcm_dist_correct(ffcm_handle* h, void* V, int32_t memory, void* stream) {
+    g_err.clear();
+    TRY(check_handle(h));
+    if (!h->distributed) return fail(FFCM_ERR_STATE, "not a rank of a z-slab decomposition (ffcm_dist_create)");
+    TRY(check_args(h->device, memory, {V}));
+    if (!V) return fail(FFCM_ERR_ARGUMENT, "V must not be NULL");
+    DeviceGuard g(h->device);
+    cudaStream_t s = h->pick(stream);
+    EngineBase* e = h->eng.get();
+    if (memory == FFCM_DEVICE) return e->dist_correct(V, s);
+    TRY(e->dist_correct(e->V_out(), s));
+    {
+        StageScope sc(h, FFCM_STAGE_D2H, s);
+        CUDA_TRY(cudaMemcpyAsync(V, e->V_out(), 3 * (size_t)h->N * h->esize, cudaMemcpyDeviceToHost, s));
+    }
+    return finish(h, s);
 }
 
 int ffcm_destroy(ffcm_handle* h) {
@@ -1673,7 +1989,7 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
                   int64_t yc, const void* F, int64_t fr, int64_t fc, int32_t memory,
                   void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     h->ckpt = false;
     h->positions = false;
     TRY(check_args(h->device, memory, {V, Y, F}));
@@ -1716,7 +2032,7 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
 
 int ffcm_wrap_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     h->ckpt = false;
     h->positions = false;
     TRY(check_args(h->device, memory, {Y}));
@@ -1735,7 +2051,7 @@ int ffcm_wrap_positions(ffcm_handle* h, const void* Y, int32_t memory, void* str
 
 int ffcm_assign_cells(ffcm_handle* h, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     h->ckpt = false;
     h->positions = false;
     DeviceGuard g(h->device);
@@ -1744,7 +2060,7 @@ int ffcm_assign_cells(ffcm_handle* h, void* stream) {
 
 int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     h->ckpt = false;
     h->positions = false;
     TRY(check_args(h->device, memory, {F}));
@@ -1763,7 +2079,7 @@ int ffcm_sort_particles_by_cell(ffcm_handle* h, const void* F, int32_t memory, v
 
 int ffcm_spread_forces(ffcm_handle* h, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     h->ckpt = false;
     h->positions = false;
     DeviceGuard g(h->device);
@@ -1772,7 +2088,7 @@ int ffcm_spread_forces(ffcm_handle* h, void* stream) {
 
 int ffcm_stokes_solve(ffcm_handle* h, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     h->ckpt = false;
     h->positions = false;
     DeviceGuard g(h->device);
@@ -1781,7 +2097,7 @@ int ffcm_stokes_solve(ffcm_handle* h, void* stream) {
 
 int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {V}));
     if (!V) return fail(FFCM_ERR_ARGUMENT, "V must not be NULL");
     DeviceGuard g(h->device);
@@ -1795,7 +2111,7 @@ int ffcm_interpolate_velocities(ffcm_handle* h, void* V, int32_t memory, void* s
 
 int ffcm_correct_velocities(ffcm_handle* h, void* V, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {V}));
     if (!V) return fail(FFCM_ERR_ARGUMENT, "V must not be NULL");
     DeviceGuard g(h->device);
@@ -1811,7 +2127,7 @@ int ffcm_correct_velocities(ffcm_handle* h, void* V, int32_t memory, void* strea
 int ffcm_mobility_checkpoint(ffcm_handle* h, void* V, const void* Y, const void* F, int32_t memory,
                              void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {V, Y, F}));
     h->ckpt = false;
     h->positions = false;
@@ -1850,7 +2166,7 @@ int ffcm_mobility_checkpoint(ffcm_handle* h, void* V, const void* Y, const void*
 
 int ffcm_adjoint(ffcm_handle* h, void* dJdY, void* dJdF, const void* lambda, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {dJdY, dJdF, lambda}));
     if (!dJdY || !dJdF || !lambda) return fail(FFCM_ERR_ARGUMENT, "dJdY, dJdF and lambda must not be NULL");
     if (!h->ckpt)
@@ -1878,7 +2194,7 @@ int ffcm_adjoint(ffcm_handle* h, void* dJdY, void* dJdF, const void* lambda, int
 int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, void* V, const void* Y,
                             const void* F, const void* V_target, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {J, dJdY, dJdF, V, Y, F, V_target}));
     h->ckpt = false;
     h->positions = false;
@@ -1928,7 +2244,7 @@ int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, v
 
 int ffcm_set_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {Y}));
     h->ckpt = false;
     h->positions = false;
@@ -1955,7 +2271,7 @@ int ffcm_set_positions(ffcm_handle* h, const void* Y, int32_t memory, void* stre
 
 int ffcm_mobility_apply(ffcm_handle* h, void* V, const void* F, int32_t memory, void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {V, F}));
     if (!V || !F) return fail(FFCM_ERR_ARGUMENT, "V and F must not be NULL");
     if (!h->positions)
@@ -1990,7 +2306,7 @@ int ffcm_cg_solve(ffcm_handle* h, void* F, const void* V, int32_t memory, double
                   int32_t maxiter, int32_t flags, int32_t* iterations, double* residual, int32_t* cg_status,
                   void* stream) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {F, V}));
     if (!F || !V) return fail(FFCM_ERR_ARGUMENT, "F and V must not be NULL");
     if (flags & ~FFCM_CG_INITIAL_GUESS) return fail(FFCM_ERR_ARGUMENT, "unknown flag bits");
@@ -2162,7 +2478,7 @@ int buffer_io(ffcm_handle* h, Engine<T>* e, int32_t which, void* ext, int64_t nb
 int buffer_dispatch(ffcm_handle* h, int32_t which, void* ext, int64_t nbytes, int32_t memory,
                     void* stream, bool get) {
     g_err.clear();
-    TRY(check_handle(h));
+    TRY(check_whole(h));
     TRY(check_args(h->device, memory, {ext}));
     if (!ext) return fail(FFCM_ERR_ARGUMENT, "buffer pointer must not be NULL");
     DeviceGuard g(h->device);

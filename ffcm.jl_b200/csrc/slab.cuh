@@ -43,8 +43,12 @@ struct SlabGeom {
     int m0, m1, m2;   // cell grid
     double cs1, cs2;  // cell sizes (y, z)
     double h;         // grid spacing
-    int nty, ntz;     // slabs along y and z
+    int nty, ntz;     // slabs along y and z (z: the slabs this grid holds)
     int lcap;         // capacity of a slab's stored particle list
+    // z slabs [zs0, zs0 + ntz) of the grid, held as mz_loc z planes of the
+    // spectrum (one GPU: zs0 = 0, mz_loc = Mz; a rank of a z-slab decomposition
+    // holds its own planes only)
+    int zs0, mz_loc;
 };
 
 // Row pitch (in T) of a slab row: holds Mx reals and, during the FFT, the
@@ -200,7 +204,7 @@ __global__ void k_slab_lists(const vec4<T>* __restrict__ Ys, const int32_t* __re
     const int lane = threadIdx.x & 31;
     const int slab = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (slab >= g.nty * g.ntz) return;   // whole warps leave together
-    const int y0r = (slab % g.nty) * BY, z0r = (slab / g.nty) * BZ;
+    const int y0r = (slab % g.nty) * BY, z0r = (slab / g.nty + g.zs0) * BZ;
     const SlabRows rows = slab_rows<BY, BZ>(g, y0r, z0r);
     int* out = lists + (int64_t)slab * g.lcap;
     const unsigned lt = (1u << lane) - 1u;
@@ -279,7 +283,7 @@ __device__ __forceinline__ void spread_put(const StencilParams<T>& p, SpreadWin<
 template <typename T, int H, int BY, int BZ>
 __device__ __forceinline__ void slab_x_r2c(T* acc, cplx<T>* __restrict__ spec, int hxp,
                                            const StencilParams<T>& p, const cplx<T>* tw, cplx<T>* dummy,
-                                           int y0r, int z0r) {
+                                           int y0r, int zl0, int mz_loc) {
     constexpr int Mx = 2 * H, P = slab_pitch(Mx), NRP = BY * BZ, ROWS = 3 * NRP;
     (void)Mx;
     if constexpr (sizeof(T) == 4 && (H == 64 || H == 128 || H == 256)) {
@@ -299,7 +303,7 @@ __device__ __forceinline__ void slab_x_r2c(T* acc, cplx<T>* __restrict__ spec, i
             fft_16xL<T, L>(v, t, rowc, tw, 2, false);
             const int c = r / NRP, bd = r % NRP;
             const int b = bd % BY, d = bd / BY;
-            cplx<T>* dst = spec + (((int64_t)c * p.Mz + z0r + d) * p.My + y0r + b) * hxp;
+            cplx<T>* dst = spec + (((int64_t)c * mz_loc + zl0 + d) * p.My + y0r + b) * hxp;
 #pragma unroll
             for (int q = 0; q < 16; ++q) {
                 const int k = t + L * q;
@@ -339,7 +343,7 @@ __device__ __forceinline__ void slab_x_r2c(T* acc, cplx<T>* __restrict__ spec, i
         if (active) {
             const int c = r / NRP, bd = r % NRP;
             const int b = bd % BY, d = bd / BY;
-            cplx<T>* dst = spec + (((int64_t)c * p.Mz + z0r + d) * p.My + y0r + b) * hxp;
+            cplx<T>* dst = spec + (((int64_t)c * mz_loc + zl0 + d) * p.My + y0r + b) * hxp;
 #pragma unroll
             for (int qq = 0; qq < 8; ++qq) {
                 const int k = j + qq * Q;
@@ -376,7 +380,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
     // FFT twiddles in shared memory, after the window / idle-lane line
     cplx<T>* tw = reinterpret_cast<cplx<T>*>(reinterpret_cast<unsigned char*>(&W) + spread_win_bytes<T, BY, BZ, H>());
     load_table(tw, twx, Mx);
-    const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
+    const int y0r = blockIdx.x * BY, z0r = (blockIdx.y + g.zs0) * BZ;
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
     // the first window stores its sums (every grid point of every row is
     // owned by one thread), later windows add; a slab without particles is
@@ -540,7 +544,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
         for (int i = threadIdx.x; i < ROWS * P; i += blockDim.x) acc[i] = T(0);
         __syncthreads();
     }
-    slab_x_r2c<T, H, BY, BZ>(acc, spec, hxp, p, tw, dummy, y0r, z0r);
+    slab_x_r2c<T, H, BY, BZ>(acc, spec, hxp, p, tw, dummy, y0r, z0r - g.zs0 * BZ, g.mz_loc);
 }
 
 // ---- x-c2r of a slab into shared memory, then gather partial velocities ----
@@ -576,7 +580,8 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
     cplx<T>* dummy = reinterpret_cast<cplx<T>*>(acc + ROWS * P);
     cplx<T>* tw = dummy + padded_len(H);   // FFT twiddles in shared memory
     load_table(tw, twx, Mx);
-    const int y0r = blockIdx.x * BY, z0r = blockIdx.y * BZ;
+    const int y0r = blockIdx.x * BY, z0r = (blockIdx.y + g.zs0) * BZ;
+    const int zl0 = z0r - g.zs0 * BZ;   // first z plane of the slab in the planes held
     const int cta = blockIdx.x + blockIdx.y * gridDim.x;
     // the slab's spectrum rows arrive by bulk copies, rows [0, R1) on bar[0]
     // and the rest on bar[1] (row starts are 16-byte aligned: the spectrum
@@ -588,7 +593,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_interp_slab(con
         if (R1 < ROWS) mbar_arrive_expect(&bar[1], (ROWS - R1) * RB);
         for (int r = 0; r < ROWS; ++r) {
             const int c = r / NRP, bd = r % NRP;
-            const cplx<T>* src = spec + (((int64_t)c * p.Mz + z0r + bd / BY) * p.My + y0r + bd % BY) * hxp;
+            const cplx<T>* src = spec + (((int64_t)c * g.mz_loc + zl0 + bd / BY) * p.My + y0r + bd % BY) * hxp;
             bulk_load(acc + r * P, src, RB, r < R1 ? &bar[0] : &bar[1]);
         }
     }

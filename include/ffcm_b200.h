@@ -323,6 +323,47 @@ int ffcm_adjoint(ffcm_handle* h, void* dJdY, void* dJdF, const void* lambda, int
 int ffcm_objective_gradient(ffcm_handle* h, double* J, void* dJdY, void* dJdF, void* V, const void* Y,
                             const void* F, const void* V_target, int32_t memory, void* stream);
 
+/* ---- one system over several GPUs (z-slab decomposition) -------------------
+ * For grids beyond one GPU's memory: R ranks (one process and GPU each) share
+ * one system. Rank r holds the z planes [z_begin, z_end) of the grid (whole
+ * spread slabs) for the spread, the y passes and the interpolation, and the
+ * kx columns [kx_begin, kx_end) of every plane for the z pass and the
+ * projector; the particles (24 bytes each) are replicated on every rank. The
+ * library never communicates: the host moves the data with its own
+ * collectives (NCCL through torch.distributed, MPI, ...) between the calls:
+ *
+ *   ffcm_dist_forward      cell list, own slabs' spread, y forward; fills the
+ *                          send buffer with R equal blocks (block q for rank q)
+ *   <all-to-all>           recv block q <- rank q's send block r
+ *   ffcm_dist_stokes       z pass + projector on the own kx columns; fills
+ *                          the send buffer again
+ *   <all-to-all>           the same exchange
+ *   ffcm_dist_interpolate  y inverse, own slabs' interpolation into the
+ *                          partial buffer (3N, this rank's share)
+ *   <all-reduce, sum>      of the partial buffer over the ranks
+ *   ffcm_dist_correct      V = h^3 partial + pair correction (every rank
+ *                          computes all N velocities)
+ *
+ * The result equals ffcm_mobility's to round-off (the sums are the same, in
+ * another order). No reference counterpart (the reference solves one system
+ * per GPU); the ranges below are contiguous and as even as possible.
+ * ffcm_dist_partition: ranges[4] = {z_begin, z_end, kx_begin, kx_end} of a
+ * rank (host only, no device work). ffcm_dist_buffers: device pointers of the
+ * send and receive buffers (R blocks of block_bytes each), of the partial
+ * buffer, and the rank's ranges; any output may be NULL. A distributed handle
+ * accepts only these calls (and ffcm_get_info, ffcm_destroy, profiling). */
+int ffcm_dist_partition(int32_t dtype, const int32_t* num_grid_points, int32_t nranks, int32_t rank,
+                        int32_t* ranges);
+int ffcm_dist_create(ffcm_handle** out, int32_t dtype, const double* L, double R_c, int64_t N, double a,
+                     double kernel_widths_ratio, const int32_t* num_grid_points, int32_t M_G, double viscosity,
+                     int32_t nranks, int32_t rank, int32_t device);
+int ffcm_dist_buffers(const ffcm_handle* h, void** send, void** recv, int64_t* block_bytes, void** partial,
+                      int32_t* ranges);
+int ffcm_dist_forward(ffcm_handle* h, const void* Y, const void* F, int32_t memory, void* stream);
+int ffcm_dist_stokes(ffcm_handle* h, void* stream);
+int ffcm_dist_interpolate(ffcm_handle* h, void* stream);
+int ffcm_dist_correct(ffcm_handle* h, void* V, int32_t memory, void* stream);
+
 /* ---- cell-list sort without allocation -------------------------------------
  * No counterpart in the reference. Computes the reference's cell-list buffers
  * (original_index, 1-based; cell_start and cell_end, 1-based inclusive, an
