@@ -20,7 +20,9 @@ the Julia reference cannot run on this machine) on the host cores.
 --workload selects the other measured configurations: `batched` (64
 suspensions x 16 right-hand sides in one graph launch), `adjoint` (objective
 gradient at N=100k, 256^3), `resistance` (conjugate-gradient resistance solve
-on the 512^3 system), `clustered` (N=2M in 2,000 Gaussian clusters, 1024^3).
+on the 512^3 system), `clustered` (N=2M in 2,000 Gaussian clusters, 1024^3),
+`split` (the 512^3 system as one system over all --gpus, by z slabs:
+strong scaling, two spectrum transposes over NCCL per solve).
 """
 from __future__ import annotations
 
@@ -1149,6 +1151,119 @@ def run_resistance(args, rank, world, local_rank):
     return 0
 
 
+SPLIT_METRIC = "particles/s per mobility solve of one system split over the GPUs by z slabs (N=500k, 512^3, Float32)"
+
+
+def run_split(args, rank, world, local_rank):
+    """The plain workload as ONE system over all ranks (ffcm_dist_*): each
+    rank spreads, transforms along y and interpolates its own z planes and
+    runs the z pass on its own kx columns; two spectrum transposes
+    (all_to_all over NCCL) and one sum of the interpolation shares
+    (all_reduce, 3N values) per solve. Strong scaling: the system is fixed."""
+    import torch
+    ffcm = _load_product()
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+        exchange = ffcm.TorchExchange()
+    else:
+        exchange = ffcm.LocalExchange()
+    Y, F = make_inputs()
+    N = Y.shape[0]
+    cfg = ffcm.DistributedConfig(np.float32, rank=rank, nranks=world, device=local_rank, **config_kwargs())
+    Yd, Fd = torch.from_numpy(Y).to(dev), torch.from_numpy(F).to(dev)
+    Vd = torch.empty_like(Yd)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+            torch.cuda.synchronize(dev)
+
+    def timed(fn, steps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        barrier()
+        return e0.elapsed_time(e1) / steps
+
+    def step():
+        cfg.mobility(Vd, Yd, Fd, exchange)
+
+    for _ in range(args.warmup):
+        step()
+    launches0 = cfg.launch_count()
+    with ClockSampler(local_rank) as clk:
+        ms = timed(step, args.steps)
+    launches = cfg.launch_count() - launches0
+    cfg.profile_begin()
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize(dev)
+    stages = cfg.profile_end()
+    # the exchange alone (two transposes and the sum)
+    ms_exchange = timed(lambda: (exchange.all_to_all(cfg.recv, cfg.send), exchange.all_to_all(cfg.recv, cfg.send),
+                                 exchange.all_reduce(cfg.partial)), args.steps)
+    # end to end: pinned host Y, F in and V out through the same entry points
+    Yh, Fh = torch.from_numpy(Y).pin_memory(), torch.from_numpy(F).pin_memory()
+    Vh = torch.empty_like(Yh).pin_memory()
+    cfg.mobility(Vh, Yh, Fh, exchange)
+    ms_e2e = timed(lambda: cfg.mobility(Vh, Yh, Fh, exchange), args.steps)
+    # every rank holds all N velocities: compare with the single-system solve
+    Vs = Vd.cpu().numpy()
+    if dist is not None:
+        t = torch.tensor([ms, ms_e2e, ms_exchange], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms_e2e, ms_exchange = (float(x) for x in t)
+    line = None
+    if rank == 0:
+        one = ffcm.FFCMConfig(np.float32, device=local_rank, **config_kwargs())
+        V1 = np.empty_like(Y)
+        ffcm.mobility(V1, one, Y, F)
+        one.close()
+        peak, peak_kind = measured_peak_hbm()
+        stage_ms = {k: v[0] / max(v[1], 1) for k, v in stages.items() if v[1] > 0}
+        per, solve_bytes = algorithmic_bytes()
+        # this rank's share of the grid traffic plus its transpose copies
+        mz = cfg.ranges[1] - cfg.ranges[0]
+        share = mz / work_geometry()[2][2]
+        line = {
+            "metric": SPLIT_METRIC, "value": N / (ms / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {**workload_config(), "parallelism": f"z-slab decomposition over {world} rank(s)",
+                       "ranges_rank0": list(cfg.ranges)},
+            "e2e": {"value": N / (ms_e2e / 1e3), "unit": UNIT, "ms_per_step": ms_e2e,
+                    "h2d_bytes_per_step": int(Yh.numel() * 4 + Fh.numel() * 4),
+                    "d2h_bytes_per_step": int(Vh.numel() * 4)},
+            "exchange_ms": ms_exchange,
+            "exchange_bytes_per_rank": int(2 * cfg.send.numel() * 4 + cfg.partial.numel() * 4),
+            "stage_ms": {k: round(v, 4) for k, v in stage_ms.items()},
+            "grid_share": share,
+            "rel_l2_vs_single_gpu": float(np.linalg.norm(Vs - V1) / np.linalg.norm(V1)),
+            "solve_roofline": {"algorithmic_bytes_per_rank": solve_bytes * share,
+                               "achieved_GBs": solve_bytes * share / (ms / 1e3) / 1e9,
+                               "peak": peak, "peak_source": peak_kind},
+            "clocks": clk.summary(),
+            "gpu_launches": int(launches),
+        }
+    cfg.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def cpu_adjoint_run(Y, F, Vt, threads):
     import ffcm_oracle as O
     cfg = O.OracleConfig(np.float32, **adjoint_kwargs(), fft_threads=threads)
@@ -1179,7 +1294,7 @@ def main():
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
                     help="plain workload only: no batched/adjoint/clustered sub-objects")
-    ap.add_argument("--workload", choices=["plain", "batched", "adjoint", "clustered", "resistance"], default="plain")
+    ap.add_argument("--workload", choices=["plain", "batched", "adjoint", "clustered", "resistance", "split"], default="plain")
     ap.add_argument("--grid", default=None,
                     help="Mx,My,Mz: smaller case at the same spacing and density (profiling)")
     args = ap.parse_args()
@@ -1215,6 +1330,8 @@ def main():
         return run_clustered(args, rank, world, local_rank)
     if args.workload == "resistance":
         return run_resistance(args, rank, world, local_rank)
+    if args.workload == "split":
+        return run_split(args, rank, world, local_rank)
     return run_ours(args, rank, world, local_rank)
 
 

@@ -37,7 +37,7 @@ __all__ = ["FFCMConfig", "mobility", "FFCMMobility", "FFCMBatch", "ArgumentError
            "spread_forces", "stokes_solve", "interpolate_velocities", "correct_velocities",
            "mobility_checkpoint", "adjoint", "objective_gradient", "rrule_mobility",
            "mobility_autograd", "cg", "CGHistory", "wisdom_export", "wisdom_import", "batch_offsets",
-           "pack_batch", "unpack_batch", "dist_partition", "DistributedConfig", "TorchExchange",
+           "pack_batch", "unpack_batch", "dist_partition", "DistributedConfig", "TorchExchange", "LocalExchange",
            "distributed_mobility_local"]
 
 
@@ -934,6 +934,17 @@ class TorchExchange:
         dist.all_reduce(partial, op=dist.ReduceOp.SUM, group=self.group)
 
 
+class LocalExchange:
+    """The collectives of a decomposition over one rank: the transposes are
+    copies and the sum is the identity."""
+
+    def all_to_all(self, recv, send):
+        recv.copy_(send)
+
+    def all_reduce(self, partial):
+        pass
+
+
 class DistributedConfig:
     """One rank of a configuration split over ``nranks`` GPUs by z slabs
     (``ffcm_dist_create``): the same parameters as ``FFCMConfig``, the grid
@@ -978,6 +989,17 @@ class DistributedConfig:
             self.close()
         except Exception:
             pass
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise FFCMError("configuration is closed")
+        return self._h
+
+    profile_begin = FFCMConfig.profile_begin
+    profile_end = FFCMConfig.profile_end
+    tuning = FFCMConfig.tuning
+    launch_count = FFCMConfig.launch_count
 
     # the steps, on the current torch stream
     def _stream(self):

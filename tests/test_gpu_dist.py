@@ -113,3 +113,49 @@ def test_dist_rejects_whole_system_calls_and_bad_grids(ffcm):
     rc = lib.ffcm_dist_stokes(plain.handle, None)
     assert rc != 0 and "z-slab" in ffcm._lib.last_error()
     plain.close()
+
+
+_NCCL_SCRIPT = r"""
+import datetime, os, sys
+import numpy as np, torch, torch.distributed as dist
+sys.path.insert(0, os.path.join(sys.argv[1], "tests"))
+from conftest import load_product
+from fixtures import random_cloud
+ffcm = load_product()
+os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=sys.argv[2])
+dev = torch.device("cuda", 0)
+torch.cuda.set_device(dev)
+dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60), device_id=dev)
+kw = dict(L=(40.0,) * 3, R_c=3.0, N=2000, kernel_widths_ratio=2.0, viscosity=1.0, num_grid_points=(64,) * 3, M_G=8)
+Y, F = random_cloud(np.float32, 2000, kw["L"], 7)
+c = ffcm.DistributedConfig(np.float32, rank=0, nranks=1, **kw)
+V = torch.empty(2000, 3, device=dev)
+c.mobility(V, torch.from_numpy(Y).cuda(), torch.from_numpy(F).cuda(), ffcm.TorchExchange())
+one = ffcm.FFCMConfig(np.float32, **kw)
+V1 = np.empty_like(Y)
+ffcm.mobility(V1, one, Y, F)
+err = float(np.linalg.norm(V.cpu().numpy() - V1) / np.linalg.norm(V1))
+c.close(); one.close()
+dist.destroy_process_group()
+print("REL", err)
+"""
+
+
+def test_dist_through_nccl_process_group(tmp_path):
+    """DistributedConfig.mobility with TorchExchange over a one-rank NCCL
+    process group (the collectives a multi-GPU run makes, on one GPU)."""
+    import socket
+    import subprocess
+    import sys
+    from pathlib import Path
+    root = Path(__file__).resolve().parent.parent
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    script = tmp_path / "nccl_one_rank.py"
+    script.write_text(_NCCL_SCRIPT)
+    r = subprocess.run([sys.executable, str(script), str(root), str(port)], capture_output=True, text=True,
+                       timeout=300)
+    assert r.returncode == 0, r.stderr[-2000:]
+    rel = float(r.stdout.split("REL")[-1])
+    assert rel < 2e-6
