@@ -178,7 +178,7 @@ __global__ void k_rank_gather(int n_part, const int32_t* __restrict__ key, const
         perm[dst] = n;
         const int64_t n3 = 3 * (int64_t)n;
         Ys[dst] = vec4<T>{Yw[n3], Yw[n3 + 1], Yw[n3 + 2], T(0)};
-        Fs[dst] = vec4<T>{F[n3], F[n3 + 1], F[n3 + 2], T(0)};
+        if (F) Fs[dst] = vec4<T>{F[n3], F[n3 + 1], F[n3 + 2], T(0)};   // F null: positions only
     }
 }
 

@@ -308,6 +308,10 @@ struct ffcm_handle {
     int64_t ncell = 0;
     size_t esize = 4;
     cudaStream_t stream = nullptr;
+    // host-array solves: the forces' copy runs on copy_stream while the
+    // positions are sorted (created on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_forces = nullptr;
     int* d_err = nullptr;
     int* h_err = nullptr;
     int64_t launches = 0;
@@ -1883,6 +1887,12 @@ int ffcm_destroy(ffcm_handle* h) {
     cg_release(h);
     h->eng.reset();
     for (cudaEvent_t e : h->events) cudaEventDestroy(e);
+    if (h->copy_stream) {
+        cudaStreamSynchronize(h->copy_stream);
+        cudaStreamDestroy(h->copy_stream);
+    }
+    if (h->ev_ready) cudaEventDestroy(h->ev_ready);
+    if (h->ev_forces) cudaEventDestroy(h->ev_forces);
     if (h->d_err) cudaFree(h->d_err);
     if (h->h_err) cudaFreeHost(h->h_err);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -2009,6 +2019,38 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
     const void* Yd = Y;
     const void* Fd = F;
     void* Vd = V;
+    if (memory == FFCM_HOST && e->uses_slab()) {
+        // The positions go first; the forces follow on the copy stream
+        // (after the work already queued on s, which may still read the
+        // staging buffer) while the positions are wrapped, sorted and listed
+        // per slab, which needs no forces; they are gathered into cell order
+        // once they have landed.
+        if (!h->copy_stream) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&h->ev_forces, cudaEventDisableTiming));
+        }
+        {
+            StageScope sc(h, FFCM_STAGE_H2D, s);
+            CUDA_TRY(cudaEventRecord(h->ev_ready, s));
+            CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev_ready, 0));
+            CUDA_TRY(cudaMemcpyAsync(e->F_in(), F, bytes, cudaMemcpyHostToDevice, h->copy_stream));
+            CUDA_TRY(cudaEventRecord(h->ev_forces, h->copy_stream));
+            CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));
+        }
+        TRY(e->wrap_hash(e->Y_in(), true, true, s));
+        TRY(e->sort(nullptr, s));
+        e->lists_built = false;
+        TRY(e->ensure_lists(s));
+        CUDA_TRY(cudaStreamWaitEvent(s, h->ev_forces, 0));
+        TRY(e->gather_forces(e->F_in(), s));
+        TRY(e->mobility_rest_same_positions(e->V_out(), s));
+        {
+            StageScope sc(h, FFCM_STAGE_D2H, s);
+            CUDA_TRY(cudaMemcpyAsync(V, e->V_out(), bytes, cudaMemcpyDeviceToHost, s));
+        }
+        return finish(h, s);
+    }
     if (memory == FFCM_HOST) {
         StageScope sc(h, FFCM_STAGE_H2D, s);
         CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));

@@ -230,18 +230,50 @@ __global__ void k_slab_lists(const vec4<T>* __restrict__ Ys, const int32_t* __re
     if (lane == 0) counts[slab] = total <= g.lcap ? total : -1;
 }
 
+// n values of T from / to shared memory in 16-byte loads and stores
+// (p 16-byte aligned, n * sizeof(T) a multiple of 16).
+template <typename T, int n>
+__device__ __forceinline__ void load16(const T* p, T (&v)[n]) {
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int q = 0; q < n / 4; ++q) {
+            const float4 c = reinterpret_cast<const float4*>(p)[q];
+            v[4 * q] = c.x; v[4 * q + 1] = c.y; v[4 * q + 2] = c.z; v[4 * q + 3] = c.w;
+        }
+    } else {
+#pragma unroll
+        for (int q = 0; q < n / 2; ++q) {
+            const double2 c = reinterpret_cast<const double2*>(p)[q];
+            v[2 * q] = c.x; v[2 * q + 1] = c.y;
+        }
+    }
+}
+template <typename T, int n>
+__device__ __forceinline__ void store16(T* p, const T (&v)[n]) {
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int q = 0; q < n / 4; ++q)
+            reinterpret_cast<float4*>(p)[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+    } else {
+#pragma unroll
+        for (int q = 0; q < n / 2; ++q) reinterpret_cast<double2*>(p)[q] = make_double2(v[2 * q], v[2 * q + 1]);
+    }
+}
+
 // One window of the spread: per entry the first x point of its stencil, the
 // slab rows it reaches, its x position, force, and per-row weight parts.
 template <typename T, int BY, int BZ, int H>
 struct SpreadWin {
     static constexpr int NRP = BY * BZ;
+    // per entry, read with 16-byte loads: gy gz of each slab row, then
+    // gy gz (r2y + r2z) of each row, then one 16-byte pad, so that the
+    // entries of a quarter-warp's loads start in distinct bank groups
+    static constexpr int WYZ = 2 * NRP + 16 / (int)sizeof(T);
+    static_assert((2 * NRP * sizeof(T)) % 16 == 0, "rows of an entry fill whole 16-byte chunks");
+    vec4<T> fy[SLAB_CAP];     // the force (x, y, z) and the particle's x position (w)
+    T wyz[SLAB_CAP][WYZ];
     int key[SLAB_CAP];        // first x point of the stencil, in [0, Mx)
     unsigned msk[SLAB_CAP];   // y rows hit (bits 0..7) | z rows hit (bits 8..15) | first x + 32768 (16..31)
-    T y0[SLAB_CAP];
-    T f[3][SLAB_CAP];
-    // rows padded by one element: lanes reading different entries at the same
-    // slab row then fall into different banks
-    T gyz[SLAB_CAP][NRP + 1], dyz[SLAB_CAP][NRP + 1];   // gy gz and gy gz (r2y + r2z)
     unsigned sk[SLAB_CAP];    // sort keys (key << 7 | entry), in sorted order
     int first[2 * H + 1];     // counting-sort bins: entries with key <= v
     int scan[32];
@@ -263,17 +295,16 @@ __device__ __forceinline__ void spread_put(const StencilParams<T>& p, SpreadWin<
     constexpr int NRP = BY * BZ;
     W.key[i] = wrap1(sx, 2 * H);
     W.msk[i] = m | ((unsigned)(sx + 32768) << 16);   // the stencil's first x point, offset into bits 16..31
-    W.y0[i] = y.x;
-    W.f[0][i] = f.x;
-    W.f[1][i] = f.y;
-    W.f[2][i] = f.z;
+    W.fy[i] = vec4<T>{f.x, f.y, f.z, y.x};
     T gyz[NRP], r2yz[NRP];
     row_weights<T, BY, BZ>(p, y, sy, sz, m, y0r, z0r, gyz, r2yz);
+    T w[2 * NRP];
 #pragma unroll
     for (int r = 0; r < NRP; ++r) {
-        W.gyz[i][r] = gyz[r];
-        W.dyz[i][r] = gyz[r] * r2yz[r];
+        w[r] = gyz[r];
+        w[NRP + r] = gyz[r] * r2yz[r];
     }
+    store16<T, 2 * NRP>(&W.wyz[i][0], w);
 }
 
 // x-r2c of every row of a spread slab (3 BY BZ rows of Mx reals, pitch P, in
@@ -456,21 +487,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2) k_spread_slab(con
                     const int i = (int)(v & 127u);
                     int e = x - (int)(v >> 7);
                     if (e < 0) e += Mx;
-                    const T y0 = W.y0[i];
+                    const vec4<T> fy = W.fy[i];
+                    const T y0 = fy.w;
                     const unsigned m = W.msk[i];
                     const int gx0 = (int)(m >> 16) - 32768;
                     T gxe, r2xe;
                     axis_weight(p, gx0 + e, y0, gxe, r2xe);
                     // (a0 + a2 (r2x + r2yz)) gx gyz = [gx (a0 + a2 r2x)] gyz + [a2 gx] [gyz r2yz]
                     const T wa = gxe * (p.a0 + p.a2 * r2xe), wc = p.a2 * gxe;
-                    const T f0 = W.f[0][i], f1 = W.f[1][i], f2 = W.f[2][i];
+                    const T f0 = fy.x, f1 = fy.y, f2 = fy.z;
+                    T w[2 * NRP];
+                    load16<T, 2 * NRP>(&W.wyz[i][0], w);
                     // rows the entry does not reach carry gyz = dyz = 0 and add nothing
 #pragma unroll
                     for (int d = 0; d < BZ; ++d)
 #pragma unroll
                         for (int b = 0; b < BY; ++b) {
                             const int r = d * BY + b;
-                            const T wgt = wa * W.gyz[i][r] + wc * W.dyz[i][r];
+                            const T wgt = wa * w[r] + wc * w[NRP + r];
                             a[0][r] += wgt * f0;
                             a[1][r] += wgt * f1;
                             a[2][r] += wgt * f2;

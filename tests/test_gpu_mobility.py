@@ -406,7 +406,14 @@ def test_float64_stencil_follows_float64(ffcm, name):
     ora = O.OracleConfig(np.float32, stencil="float64", **kw)
     assert rel_l2(Vg, O.apply(ora, z["f32_Y"], z["f32_F"])) < 1e-5
     V64 = z["f64_V"]
-    assert rel_l2(Vg, V64) < 1e-5 and rel_l2(Vg, V64) <= rel_l2(Vr, V64) * 1.01
+    e_geo, e_ref = rel_l2(Vg, V64), rel_l2(Vr, V64)
+    assert e_geo < 1e-5
+    # below ~2e-6 both modes sit at the Float32 rounding floor of the solve
+    # (the summation order of the interpolation varies run to run); above it
+    # the reference geometry has flipped anchors, which the Float64 geometry
+    # must not have
+    if e_ref > 2e-6:
+        assert e_geo < e_ref
     # Float64 handles take the mode too and stay at Float64 accuracy
     c64 = ffcm.FFCMConfig(np.float64, stencil="float64", **kw)
     assert rel_l2(_run(ffcm, c64, z["f64_Y"], z["f64_F"]), V64) < 1e-10
