@@ -672,6 +672,8 @@ struct Engine final : EngineBase {
                 TRY(raise_smem_cap((const void*)ypipe_kernel<T>(My, B), ypipe_smem<T>(My, B)));
             if (fast_y && ytma_kernel<T>(My, B) && ytma_smem<T>(My, B) <= 226 * 1024)
                 TRY(raise_smem_cap((const void*)ytma_kernel<T>(My, B), ytma_smem<T>(My, B)));
+            if (fast_y && ytma3_kernel<T>(My, B) && ytma_smem<T>(My, B, 3) <= 226 * 1024)
+                TRY(raise_smem_cap((const void*)ytma3_kernel<T>(My, B), ytma_smem<T>(My, B, 3)));
             if (fast_z && ztma_kernel<T>(Mz, B) && ztma_smem<T>(Mz, B) <= 226 * 1024)
                 TRY(raise_smem_cap((const void*)ztma_kernel<T>(Mz, B), ztma_smem<T>(Mz, B)));
             if (fast_z && zin_kernel<T>(Mz, B) && zin_smem<T>(Mz, B) <= 226 * 1024)
@@ -825,7 +827,7 @@ struct Engine final : EngineBase {
         for (int i = 1, B = 2; B <= 16; ++i, B *= 2) {
             if (fast_z && zpitch % B == 0 && (ztma_kernel<T>(Mz, B) || zin_kernel<T>(Mz, B)))
                 zmap_ok[i] = make(&zmap[i], zbuf, zpitch, 3 * Mz, (cuuint32_t)(B * EPC), 1, (cuuint32_t)tma_zbox(Mz));
-            if (fast_y && hxp % B == 0 && ytma_kernel<T>(My, B))
+            if (fast_y && hxp % B == 0 && (ytma_kernel<T>(My, B) || ytma3_kernel<T>(My, B)))
                 ymap_ok[i] = make(&ymap[i], spec, hxp, 3 * mzl, (cuuint32_t)(B * EPC), (cuuint32_t)tma_zbox(My), 1);
         }
     }
@@ -857,7 +859,9 @@ struct Engine final : EngineBase {
                             (k == 1 && ypipe_kernel<T>(My, B) && hxp % B == 0 &&
                              ypipe_smem<T>(My, B) <= 200 * 1024 && t.ygrid >= 1) ||
                             (k == 2 && ytma_kernel<T>(My, B) && ymap_ok[log2i(B)] &&
-                             ytma_smem<T>(My, B) <= 226 * 1024 && t.ygrid >= 1);
+                             ytma_smem<T>(My, B) <= 226 * 1024 && t.ygrid >= 1) ||
+                            (k == 3 && ytma3_kernel<T>(My, B) && ymap_ok[log2i(B)] &&
+                             ytma_smem<T>(My, B, 3) <= 226 * 1024 && t.ygrid >= 1);
             if (!ok) return false;
         }
         if (fast_z) {
@@ -918,7 +922,7 @@ struct Engine final : EngineBase {
         if (fast_y) {
             float best = 1e30f;
             int bk = 0, bB = By, bg = 0;
-            for (int kind = 0; kind < 3; ++kind)
+            for (int kind = 0; kind < 4; ++kind)
                 for (int B : {2, 4, 8, 16}) {
                     if (fyk >= 0 && (kind != fyk || B != fyB)) continue;
                     if (kind == 0 && !y_kernel<T>(My, B)) continue;
@@ -926,6 +930,8 @@ struct Engine final : EngineBase {
                                        ypipe_smem<T>(My, B) <= 200 * 1024)) continue;
                     if (kind == 2 && !(ytma_kernel<T>(My, B) && ymap_ok[log2i(B)] &&
                                        ytma_smem<T>(My, B) <= 226 * 1024)) continue;
+                    if (kind == 3 && !(ytma3_kernel<T>(My, B) && ymap_ok[log2i(B)] &&
+                                       ytma_smem<T>(My, B, 3) <= 226 * 1024)) continue;
                     if (kind == 0) {
                         int cand[4];
                         const int nc = y_bundles(My, cand);
@@ -944,6 +950,11 @@ struct Engine final : EngineBase {
                         const int ntiles = ((nkx + B - 1) / B) * mzl * 3;
                         TRY(persistent_grid((const void*)ytma_kernel<T>(My, B), B * (My / 8),
                                             ytma_smem<T>(My, B), ntiles, ygrid));
+                    }
+                    if (kind == 3) {
+                        const int ntiles = ((nkx + B - 1) / B) * mzl;
+                        TRY(persistent_grid((const void*)ytma3_kernel<T>(My, B), B * (My / 8),
+                                            ytma_smem<T>(My, B, 3), ntiles, ygrid));
                     }
                     float ms = 0;
                     TRY(time_launches([&] { return launch_y(h->stream, 0); }, ms));
@@ -1393,6 +1404,12 @@ struct Engine final : EngineBase {
     // y pass over the kx columns [k0, k1) (the whole spectrum when k1 <= 0).
     int launch_y(cudaStream_t s, int inverse, int k0 = 0, int k1 = 0) {
         if (k1 <= 0) k1 = nkx;
+        if (fast_y && ykind == 3) {   // three planes per tile
+            const int ntiles = ((k1 - k0 + By - 1) / By) * mzl;
+            return launch(h, ytma3_kernel<T>(My, By), std::min(ygrid, ntiles), By * (My / 8),
+                          ytma_smem<T>(My, By, 3), s, ymap[log2i(By)], spec, k0, k1, mzl, hxp, (const cplx<T>*)twy,
+                          inverse, h->d_err);
+        }
         if (fast_y && ykind == 2) {
             const int ntiles = ((k1 - k0 + By - 1) / By) * mzl * 3;
             return launch(h, ytma_kernel<T>(My, By), std::min(ygrid, ntiles), By * (My / 8), ytma_smem<T>(My, By),
@@ -2021,10 +2038,10 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
     void* Vd = V;
     if (memory == FFCM_HOST && e->uses_slab()) {
         // The positions go first; the forces follow on the copy stream
-        // (after the work already queued on s, which may still read the
-        // staging buffer) while the positions are wrapped, sorted and listed
-        // per slab, which needs no forces; they are gathered into cell order
-        // once they have landed.
+        // (after the positions' copy and so after the work queued on s before
+        // it, which may still read the staging buffer) while the positions
+        // are wrapped, sorted and listed per slab, which needs no forces; they
+        // are gathered into cell order once they have landed.
         if (!h->copy_stream) {
             CUDA_TRY(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&h->ev_ready, cudaEventDisableTiming));
@@ -2032,11 +2049,13 @@ int ffcm_mobility(ffcm_handle* h, void* V, int64_t vr, int64_t vc, const void* Y
         }
         {
             StageScope sc(h, FFCM_STAGE_H2D, s);
+            CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));
+            // after the positions' copy (the two would otherwise share the
+            // link and the positions would land no sooner)
             CUDA_TRY(cudaEventRecord(h->ev_ready, s));
             CUDA_TRY(cudaStreamWaitEvent(h->copy_stream, h->ev_ready, 0));
             CUDA_TRY(cudaMemcpyAsync(e->F_in(), F, bytes, cudaMemcpyHostToDevice, h->copy_stream));
             CUDA_TRY(cudaEventRecord(h->ev_forces, h->copy_stream));
-            CUDA_TRY(cudaMemcpyAsync(e->Y_in(), Y, bytes, cudaMemcpyHostToDevice, s));
         }
         TRY(e->wrap_hash(e->Y_in(), true, true, s));
         TRY(e->sort(nullptr, s));

@@ -272,11 +272,22 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftr_z_stokes(
     if (threadIdx.x == 0) bulk_wait_all();
 }
 
-// y pass, same scheme: a tile is B kx columns x all n rows y of one (c, z)
-// plane (tensor coordinate z = c * Mz + z), loaded with n / min(256, n) tiled
-// copies into staging laid out [y][B].
-// block = B * n/8 threads; smem: slack | staging (n B) | table (n) | exchange (B padded_len(n)).
-template <typename T, int n, int B>
+// Complex values of one plane's exchange region of the TMA y pass: B lines
+// of padded_len(n), rounded up to 128 bytes so that every region (the
+// source of a tiled bulk store) starts on a 128-byte boundary.
+template <typename T>
+__host__ __device__ constexpr int ytma_exchange(int n, int B) {
+    return (int)(((size_t)B * padded_len(n) * sizeof(cplx<T>) + 127) / 128 * 128 / sizeof(cplx<T>));
+}
+
+// y pass, same scheme: a tile is B kx columns x all n rows y of NP
+// consecutive (c, z) planes (tensor coordinate z = c * Mz + z), each plane
+// loaded with n / min(256, n) tiled copies into its staging [y][B]. With
+// NP > 1 each thread transforms one line of every plane in lockstep (the
+// twiddles and exchange barriers of a stage serve NP lines).
+// block = B * n/8 threads; smem: slack | staging (NP n B) | table (n) |
+// exchange (NP B padded_len(n)).
+template <typename T, int n, int B, int NP = 1>
 __global__ void __launch_bounds__(B * (n / 8)) k_fftt_y(const __grid_constant__ CUtensorMap tmap,
                                                         cplx<T>* __restrict__ spec, int kx0, int kx1, int Mz,
                                                         int hxp, const cplx<T>* __restrict__ twy, int inverse,
@@ -284,32 +295,38 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_y(const __grid_constant__ 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar;
     constexpr int Q = n / 8, YB = tma_zbox(n), NCOPY = n / YB;
-    constexpr unsigned TILE_BYTES = (unsigned)(n * B * sizeof(cplx<T>));
+    constexpr unsigned TILE_BYTES = (unsigned)(NP * n * B * sizeof(cplx<T>));
+    constexpr int EXS = ytma_exchange<T>(n, B);   // one plane's exchange region
     cplx<T>* stage = reinterpret_cast<cplx<T>*>(smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u));
-    cplx<T>* tw = stage + n * B;
+    cplx<T>* tw = stage + NP * n * B;
     cplx<T>* ex_sm = tw + n;
     load_table(tw, twy, n);
     const int b = threadIdx.x % B, j = threadIdx.x / B;
     const int tiles_x = (kx1 - kx0 + B - 1) / B;
-    const int ntiles = tiles_x * Mz * 3;
+    const int ntiles = tiles_x * (Mz * 3 / NP);
     auto issue = [&](int t) {   // one thread, after a barrier
-        const int tx = t % tiles_x, pz = t / tiles_x;
+        const int tx = t % tiles_x, pz = (t / tiles_x) * NP;
         fence_proxy_async_smem();   // the block's reads of the staging buffer come first
         mbar_arrive_expect(&bar, TILE_BYTES);
 #pragma unroll
-        for (int k = 0; k < NCOPY; ++k)
-            tma_load_3d(stage + k * YB * B, &tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, k * YB, pz, &bar);
+        for (int pl = 0; pl < NP; ++pl)
+#pragma unroll
+            for (int k = 0; k < NCOPY; ++k)
+                tma_load_3d(stage + (pl * NCOPY + k) * YB * B, &tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX,
+                            k * YB, pz + pl, &bar);
     };
     if (threadIdx.x == 0) {
         mbar_init(&bar, 1);
         if ((int)blockIdx.x < ntiles) issue(blockIdx.x);
     }
     __syncthreads();
-    const Exchange<T> ex[1] = {Exchange<T>{ex_sm, b, B}};
-    // the result tile leaves through the exchange region ([y][B], 128-byte
-    // aligned) by tiled bulk stores
-    cplx<T>* out = ex_sm;
-    static_assert(n * B <= B * padded_len(n), "the result tile must fit the exchange region");
+    Exchange<T> ex[NP];
+#pragma unroll
+    for (int pl = 0; pl < NP; ++pl) ex[pl] = Exchange<T>{ex_sm + pl * EXS, b, B};
+    // the result tiles leave through the exchange regions ([y][B] per plane,
+    // 128-byte aligned) by tiled bulk stores
+    static_assert(n * B <= EXS, "a result tile must fit its exchange region");
+    static_assert((EXS * sizeof(cplx<T>)) % 128 == 0, "exchange regions start on 128-byte boundaries");
     unsigned phase = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, phase ^= 1u) {
         const bool landed = mbar_wait_bounded(&bar, phase, 1 << 22);
@@ -321,23 +338,30 @@ __global__ void __launch_bounds__(B * (n / 8)) k_fftt_y(const __grid_constant__ 
             mbar_wait_bounded(&bar, phase, 1 << 22);
             return;
         }
-        cplx<T> v[1][8];
+        cplx<T> v[NP][8];
 #pragma unroll
-        for (int q = 0; q < 8; ++q) v[0][q] = stage[(j + q * Q) * B + b];
-        if (threadIdx.x == 0) bulk_wait_read_all();   // the previous tile's stores left the exchange region
+        for (int pl = 0; pl < NP; ++pl)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) v[pl][q] = stage[pl * n * B + (j + q * Q) * B + b];
+        if (threadIdx.x == 0) bulk_wait_read_all();   // the previous tile's stores left the exchange regions
         __syncthreads();   // the staging buffer is free for the next tile
         if (threadIdx.x == 0 && t + (int)gridDim.x < ntiles) issue(t + gridDim.x);
-        fft_lines_lockstep<T, n, 1>(v, j, ex, tw, inverse != 0);
-        const int tx = t % tiles_x, pz = t / tiles_x;
+        fft_lines_lockstep<T, n, NP>(v, j, ex, tw, inverse != 0);
+        const int tx = t % tiles_x, pz = (t / tiles_x) * NP;
         __syncthreads();   // every exchange read of the transform is done
 #pragma unroll
-        for (int q = 0; q < 8; ++q) out[(j + q * Q) * B + b] = v[0][q];
+        for (int pl = 0; pl < NP; ++pl)
+#pragma unroll
+            for (int q = 0; q < 8; ++q) ex_sm[pl * EXS + (j + q * Q) * B + b] = v[pl][q];
         fence_proxy_async_smem();
         __syncthreads();
         if (threadIdx.x == 0) {
 #pragma unroll
-            for (int k = 0; k < NCOPY; ++k)
-                tma_store_3d(&tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, k * YB, pz, out + k * YB * B);
+            for (int pl = 0; pl < NP; ++pl)
+#pragma unroll
+                for (int k = 0; k < NCOPY; ++k)
+                    tma_store_3d(&tmap, (kx0 + tx * B) * TmaElem<T>::PER_CPLX, k * YB, pz + pl,
+                                 ex_sm + pl * EXS + k * YB * B);
             bulk_commit();
         }
     }
@@ -348,8 +372,22 @@ template <typename T>
 using YTmaKernel = void (*)(const CUtensorMap, cplx<T>*, int, int, int, int, const cplx<T>*, int, int*);
 
 template <typename T>
-size_t ytma_smem(int n, int B) {
-    return 128 + (size_t)(n * B + n + B * padded_len(n)) * sizeof(cplx<T>);
+size_t ytma_smem(int n, int B, int NP = 1) {
+    return 128 + (size_t)(NP * n * B + n + NP * ytma_exchange<T>(n, B)) * sizeof(cplx<T>);
+}
+
+// y pass with three planes per tile (autotuner kind 3), per (n, B).
+template <typename T>
+YTmaKernel<T> ytma3_kernel(int n, int B) {
+#define FFCM_Y3(NN, BB) if (n == NN && B == BB) return k_fftt_y<T, NN, BB, 3>;
+    // the instantiations that fit their register budget without spills
+    if constexpr (sizeof(T) == 4) {
+        FFCM_Y3(256, 4) FFCM_Y3(512, 4) FFCM_Y3(512, 8) FFCM_Y3(1024, 4)
+    } else {
+        FFCM_Y3(256, 4) FFCM_Y3(256, 8) FFCM_Y3(512, 4)
+    }
+#undef FFCM_Y3
+    return nullptr;
 }
 
 template <typename T>

@@ -23,12 +23,13 @@ CASES = {"64^3": dict(L=(40.0,) * 3, N=2000, M=(64, 64, 64)),
          "64x64x1024": dict(L=(40.0, 40.0, 640.0), N=32000, M=(64, 64, 1024)),
          "64x1024x64": dict(L=(40.0, 640.0, 40.0), N=32000, M=(64, 1024, 64)),
          "1024x64x64": dict(L=(640.0, 40.0, 40.0), N=32000, M=(1024, 64, 64)),
-         # lines of 512 along y
+         # lines of 512 and 256 along y (also the three-plane y pass)
          "64x512x64": dict(L=(40.0, 320.0, 40.0), N=16000, M=(64, 512, 64)),
+         "64x256x64": dict(L=(40.0, 160.0, 40.0), N=8000, M=(64, 256, 64)),
          # lines of 256 and 512 along z (the in-place wide-tile z pass)
          "64x64x256": dict(L=(40.0, 40.0, 160.0), N=8000, M=(64, 64, 256)),
          "64x64x512": dict(L=(40.0, 40.0, 320.0), N=16000, M=(64, 64, 512))}
-Y_VARIANTS = [(k, B) for k in (0, 1, 2) for B in (2, 4, 8, 16)]
+Y_VARIANTS = [(k, B) for k in (0, 1, 2, 3) for B in (2, 4, 8, 16)]
 Z_VARIANTS = [(k, B) for k in (0, 1, 2, 3, 4) for B in (2, 4, 8, 16)]
 
 
@@ -79,11 +80,12 @@ def test_z_variant(ffcm, T, case, kind, B):
 
 # (y, z) variants pinned with chunking, so that which chunk widths apply does
 # not depend on what the autotuner happens to pick
-CHUNK_PINS = {"register": ("0,8", "0,8"), "pipelined": ("1,8", "1,4"), "tma": ("2,8", "3,8")}
+CHUNK_PINS = {"register": ("0,8", "0,8"), "pipelined": ("1,8", "1,4"), "tma": ("2,8", "3,8"),
+              "tma3": ("3,4", "3,8")}
 
 
 @pytest.mark.parametrize("T", [np.float32, np.float64])
-@pytest.mark.parametrize("case", ["64^3", "128^3"])
+@pytest.mark.parametrize("case", ["64^3", "128^3", "64x256x64"])
 @pytest.mark.parametrize("chunk", [8, 16, 32])
 @pytest.mark.parametrize("pin", list(CHUNK_PINS))
 def test_chunked_yz(ffcm, T, case, chunk, pin):
