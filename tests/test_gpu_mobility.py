@@ -355,6 +355,40 @@ def test_clustered_suspension_matches_oracle(ffcm, T):
 
 
 @pytest.mark.parametrize("T", TS)
+@pytest.mark.parametrize("N,L,M", [(5000, 12.0, 32), (3000, 40.0, 64)])
+def test_crowded_cell_correction_matches_oracle(ffcm, T, N, L, M):
+    """Crowded cells in the pair correction: 64 cells of ~78 particles
+    each, and a uniform background with one tight cluster. Same pairs and
+    sums as the oracle, through the fused solve and through the step API's
+    correct_velocities."""
+    rng = np.random.default_rng(N)
+    if L < 20:
+        Y = (rng.random((N, 3)) * L).astype(T)
+    else:
+        Y = (rng.random((N, 3)) * L).astype(T)
+        Y[:600] = (L / 2 + rng.standard_normal((600, 3)) * 1.5).astype(T)
+    F = rng.standard_normal((N, 3)).astype(T)
+    prod, ora = both(ffcm, T, **kw_of(L, N, M, R_c=3.0))
+    V = np.empty_like(Y)
+    ffcm.mobility(V, prod, Y, F)
+    Vo = O.apply(ora, Y, F)
+    tol = 1e-5 if T == np.float32 else 1e-10
+    assert rel_l2(V, Vo) < tol
+    # the correction alone (step API, V += correction from zero)
+    ffcm.wrap_positions(prod, Y)
+    ffcm.assign_cells(prod)
+    ffcm.sort_particles_by_cell(prod, F)
+    Vc = np.zeros_like(Y)
+    ffcm.correct_velocities(Vc, prod)
+    Yw = np.empty_like(Y)
+    O.wrap_positions(Yw, Y, ora.L)
+    O.assign_cells(ora, Yw)
+    O.sort_particles_by_cell(ora, Yw, F)
+    Vco = O.correct_velocities(np.zeros_like(Y), ora)
+    assert rel_l2(Vc, Vco) < tol
+
+
+@pytest.mark.parametrize("T", TS)
 def test_fixed_position_operator_on_cuda_tensors(ffcm, T):
     """M @ F and mul! on CUDA tensors (the zero-copy device path of
     FFCMMobility) agree with the host-array path and with the oracle."""
