@@ -68,6 +68,70 @@ __device__ __forceinline__ T min_image(T x, T L) {
 // interpolation, which left its sums in sorted order in Vs).
 inline int corr_tpp(int64_t n_part) { return n_part <= 200000 ? 4 : 1; }
 
+// Self term plus the pair terms of sorted particle s over its 27 neighbour
+// cells; lane `sub` of the particle's TPP-lane group takes cells q = sub,
+// sub + TPP, ... of the reference's order, and after the shuffles every lane
+// of the group holds the group's sum.
+template <typename T, int TPP>
+__device__ __forceinline__ void pair_velocity(int s, int sub, unsigned group, const vec4<T>* __restrict__ Ys,
+                                              const vec4<T>* __restrict__ Fs, const int32_t* __restrict__ off,
+                                              const CorrConsts<T>& c, T& v0, T& v1, T& v2) {
+    const vec4<T> yn = Ys[s];
+    const vec4<T> fn = Fs[s];
+    int cx = (int)floor_t(mul_rn(yn.x, c.ic0));
+    int cy = (int)floor_t(mul_rn(yn.y, c.ic1));
+    int cz = (int)floor_t(mul_rn(yn.z, c.ic2));
+    cx = max(0, min(cx, c.m0 - 1));
+    cy = max(0, min(cy, c.m1 - 1));
+    cz = max(0, min(cz, c.m2 - 1));
+    v0 = 0;
+    v1 = 0;
+    v2 = 0;
+    if (sub == 0) {
+        v0 = c.self * fn.x;
+        v1 = c.self * fn.y;
+        v2 = c.self * fn.z;
+    }
+    auto visit = [&](int nx, int ny, int nz) {
+        const int cn = nx + (ny + nz * c.m1) * c.m0;
+        const int e = off[cn + 1];
+        for (int s2 = off[cn]; s2 < e; ++s2) {
+            if (s2 == s) continue;
+            const vec4<T> ym = Ys[s2];
+            const T x0 = min_image(sub_rn(yn.x, ym.x), c.L0);
+            const T x1 = min_image(sub_rn(yn.y, ym.y), c.L1);
+            const T x2 = min_image(sub_rn(yn.z, ym.z), c.L2);
+            const T rr = add_rn(add_rn(mul_rn(x0, x0), mul_rn(x1, x1)), mul_rn(x2, x2));
+            if (!(rr < c.Rc2)) continue;
+            T A, B;
+            correction_scalars(sqrt_t(rr), c, A, B);
+            const vec4<T> fm = Fs[s2];
+            const T xF = x0 * fm.x + x1 * fm.y + x2 * fm.z;
+            const T bx = B * xF;
+            v0 += A * fm.x + bx * x0;
+            v1 += A * fm.y + bx * x1;
+            v2 += A * fm.z + bx * x2;
+        }
+    };
+    if constexpr (TPP == 1) {
+        // the reference's dz / dy / dx loop order
+        for (int dz = -1; dz <= 1; ++dz)
+            for (int dy = -1; dy <= 1; ++dy)
+                for (int dx = -1; dx <= 1; ++dx)
+                    visit(imod(cx + dx, c.m0), imod(cy + dy, c.m1), imod(cz + dz, c.m2));
+    } else {
+        // cell q of that order goes to lane q mod TPP
+        for (int q = sub; q < 27; q += TPP)
+            visit(imod(cx + q % 3 - 1, c.m0), imod(cy + (q / 3) % 3 - 1, c.m1), imod(cz + q / 9 - 1, c.m2));
+    }
+#pragma unroll
+    for (int o = 1; o < TPP; o <<= 1) {
+        v0 += __shfl_xor_sync(group, v0, o);
+        v1 += __shfl_xor_sync(group, v1, o);
+        v2 += __shfl_xor_sync(group, v2, o);
+    }
+}
+
 template <typename T, int TPP>
 __global__ void k_correct(int n_part, const vec4<T>* __restrict__ Ys,
                           const vec4<T>* __restrict__ Fs, const int32_t* __restrict__ off,
@@ -79,58 +143,8 @@ __global__ void k_correct(int n_part, const vec4<T>* __restrict__ Ys,
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n_part * TPP;
          t += nthreads) {
         const int s = (int)(t / TPP);
-        const vec4<T> yn = Ys[s];
-        const vec4<T> fn = Fs[s];
-        int cx = (int)floor_t(mul_rn(yn.x, c.ic0));
-        int cy = (int)floor_t(mul_rn(yn.y, c.ic1));
-        int cz = (int)floor_t(mul_rn(yn.z, c.ic2));
-        cx = max(0, min(cx, c.m0 - 1));
-        cy = max(0, min(cy, c.m1 - 1));
-        cz = max(0, min(cz, c.m2 - 1));
-        T v0 = 0, v1 = 0, v2 = 0;
-        if (sub == 0) {
-            v0 = c.self * fn.x;
-            v1 = c.self * fn.y;
-            v2 = c.self * fn.z;
-        }
-        auto visit = [&](int nx, int ny, int nz) {
-            const int cn = nx + (ny + nz * c.m1) * c.m0;
-            const int e = off[cn + 1];
-            for (int s2 = off[cn]; s2 < e; ++s2) {
-                if (s2 == s) continue;
-                const vec4<T> ym = Ys[s2];
-                const T x0 = min_image(sub_rn(yn.x, ym.x), c.L0);
-                const T x1 = min_image(sub_rn(yn.y, ym.y), c.L1);
-                const T x2 = min_image(sub_rn(yn.z, ym.z), c.L2);
-                const T rr = add_rn(add_rn(mul_rn(x0, x0), mul_rn(x1, x1)), mul_rn(x2, x2));
-                if (!(rr < c.Rc2)) continue;
-                T A, B;
-                correction_scalars(sqrt_t(rr), c, A, B);
-                const vec4<T> fm = Fs[s2];
-                const T xF = x0 * fm.x + x1 * fm.y + x2 * fm.z;
-                const T bx = B * xF;
-                v0 += A * fm.x + bx * x0;
-                v1 += A * fm.y + bx * x1;
-                v2 += A * fm.z + bx * x2;
-            }
-        };
-        if constexpr (TPP == 1) {
-            // the reference's dz / dy / dx loop order
-            for (int dz = -1; dz <= 1; ++dz)
-                for (int dy = -1; dy <= 1; ++dy)
-                    for (int dx = -1; dx <= 1; ++dx)
-                        visit(imod(cx + dx, c.m0), imod(cy + dy, c.m1), imod(cz + dz, c.m2));
-        } else {
-            // cell q of that order goes to lane q mod TPP
-            for (int q = sub; q < 27; q += TPP)
-                visit(imod(cx + q % 3 - 1, c.m0), imod(cy + (q / 3) % 3 - 1, c.m1), imod(cz + q / 9 - 1, c.m2));
-        }
-#pragma unroll
-        for (int o = 1; o < TPP; o <<= 1) {
-            v0 += __shfl_xor_sync(group, v0, o);
-            v1 += __shfl_xor_sync(group, v1, o);
-            v2 += __shfl_xor_sync(group, v2, o);
-        }
+        T v0, v1, v2;
+        pair_velocity<T, TPP>(s, sub, group, Ys, Fs, off, c, v0, v1, v2);
         if (sub == 0) {
             const int64_t n = perm[s];
             if (Vs) {
@@ -143,6 +157,42 @@ __global__ void k_correct(int n_part, const vec4<T>* __restrict__ Ys,
                 V[3 * n + 2] += v2;
             }
         }
+    }
+}
+
+// The pair terms alone, dv[3 s + c] in sorted order, for a solve that runs
+// them on a second stream beside its grid stages (they need only the sorted
+// particles and the cell list); k_finish_velocity then adds the
+// interpolation sums, with the same arithmetic as k_correct.
+template <typename T, int TPP>
+__global__ void k_correct_pairs(int n_part, const vec4<T>* __restrict__ Ys, const vec4<T>* __restrict__ Fs,
+                                const int32_t* __restrict__ off, CorrConsts<T> c, T* __restrict__ dv) {
+    const int sub = threadIdx.x % TPP;
+    const unsigned group = ((1u << TPP) - 1u) << (lane_id() & ~(TPP - 1));
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < (int64_t)n_part * TPP;
+         t += nthreads) {
+        const int s = (int)(t / TPP);
+        T v0, v1, v2;
+        pair_velocity<T, TPP>(s, sub, group, Ys, Fs, off, c, v0, v1, v2);
+        if (sub == 0) {
+            dv[3 * (int64_t)s] = v0;
+            dv[3 * (int64_t)s + 1] = v1;
+            dv[3 * (int64_t)s + 2] = v2;
+        }
+    }
+}
+
+// V[:, perm[s]] = h^3 Vs[s] + dv[s].
+template <typename T>
+__global__ void k_finish_velocity(int n_part, const int32_t* __restrict__ perm, const T* __restrict__ Vs,
+                                  const T* __restrict__ dv, T h3, T* __restrict__ V) {
+    const int64_t nthreads = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < n_part; s += nthreads) {
+        const int64_t n = perm[s];
+        V[3 * n] = h3 * Vs[3 * s] + dv[3 * s];
+        V[3 * n + 1] = h3 * Vs[3 * s + 1] + dv[3 * s + 1];
+        V[3 * n + 2] = h3 * Vs[3 * s + 2] + dv[3 * s + 2];
     }
 }
 

@@ -312,6 +312,13 @@ struct ffcm_handle {
     // positions are sorted (created on first use)
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_ready = nullptr, ev_forces = nullptr;
+    // fused solves outside stream capture: the pair correction runs on
+    // side_stream beside the grid stages (fork after the spread, join before
+    // the last kernel; created on first use). FFCM_OVERLAP_PAIRS=0 keeps it
+    // on the solve's stream.
+    bool overlap_pairs = true;
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int* d_err = nullptr;
     int* h_err = nullptr;
     int64_t launches = 0;
@@ -473,6 +480,7 @@ struct Engine final : EngineBase {
     SlabKernels<T> sk;
     SlabGeom sg;
     T* partial = nullptr;
+    T* dvs = nullptr;            // pair terms in sorted order (side-stream correction)
     int* slab_lists = nullptr;   // per-slab particle lists kept by the spread
     int* slab_counts = nullptr;
     int ntiles;
@@ -1195,16 +1203,56 @@ struct Engine final : EngineBase {
             return correct(V, s);
         }
         TRY(spread_to_spectrum(s, nullptr, build_lists));
+        bool side = false;
+        TRY(fork_pairs(s, side));
         TRY(stokes_yz(s));
         if (keep_u) {
             StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
             TRY(x_inverse(gu, s));
         }
         TRY(interp_from_spectrum(s));
+        if (side) {
+            // (the correction stage's time is the pair kernel's, on the side stream)
+            CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
+            return launch(h, k_finish_velocity<T>, grid_for(N, 256), 256, 0, s, N, (const int32_t*)perm,
+                          (const T*)partial, (const T*)dvs, h3, static_cast<T*>(V));
+        }
         StageScope sc(h, FFCM_STAGE_CORRECT, s);
         return launch(h, corr_tpp(N) == 4 ? k_correct<T, 4> : k_correct<T, 1>, grid_for((int64_t)N * corr_tpp(N), 128), 128, 0, s, N, (const vec4<T>*)Ys,
                       (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
                       static_cast<T*>(V), cc, (const T*)partial, h3);
+    }
+
+    // The pair correction depends only on the sorted particles and the cell
+    // list, so outside stream capture it runs on the handle's side stream
+    // while the y/z passes and the interpolation run on s: the fork follows
+    // the spread (the y pass leaves a third of each SM's registers free, the
+    // spread none), the join precedes k_finish_velocity. `side` tells the
+    // caller whether it forked. Under capture (the batched graph, the CG
+    // loop) the solve keeps the single-stream order.
+    int fork_pairs(cudaStream_t s, bool& side) {
+        side = false;
+        if (!h->overlap_pairs) return FFCM_OK;
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        CUDA_TRY(cudaStreamIsCapturing(s, &cap));
+        if (cap != cudaStreamCaptureStatusNone) return FFCM_OK;
+        if (!dvs) TRY(alloc(dvs, 3 * (size_t)N));
+        if (!h->side_stream) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
+        }
+        CUDA_TRY(cudaEventRecord(h->ev_fork, s));
+        CUDA_TRY(cudaStreamWaitEvent(h->side_stream, h->ev_fork, 0));
+        {
+            StageScope sc(h, FFCM_STAGE_CORRECT, h->side_stream);
+            TRY(launch(h, corr_tpp(N) == 4 ? k_correct_pairs<T, 4> : k_correct_pairs<T, 1>,
+                       grid_for((int64_t)N * corr_tpp(N), 128), 128, 0, h->side_stream, N, (const vec4<T>*)Ys,
+                       (const vec4<T>*)Fs, (const int32_t*)off, cc, dvs));
+        }
+        CUDA_TRY(cudaEventRecord(h->ev_join, h->side_stream));
+        side = true;
+        return FFCM_OK;
     }
 
     // ---- z-slab decomposition --------------------------------------------
@@ -1776,6 +1824,10 @@ static int create_handle(ffcm_handle** out, int32_t dtype, const double* L, doub
         else if (v && *v && std::strcmp(v, "reference") != 0)
             return fail(FFCM_ERR_ARGUMENT, "FFCM_STENCIL must be \"reference\" or \"float64\"");
     }
+    {
+        const char* v = std::getenv("FFCM_OVERLAP_PAIRS");
+        if (v && std::strcmp(v, "0") == 0) h->overlap_pairs = false;
+    }
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMalloc(&h->d_err, sizeof(int)));
     CUDA_TRY(cudaMemset(h->d_err, 0, sizeof(int)));
@@ -1901,8 +1953,12 @@ int ffcm_destroy(ffcm_handle* h) {
     if (!h) return FFCM_OK;
     DeviceGuard g(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->side_stream) cudaStreamSynchronize(h->side_stream);
     cg_release(h);
     h->eng.reset();
+    if (h->side_stream) cudaStreamDestroy(h->side_stream);
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
     for (cudaEvent_t e : h->events) cudaEventDestroy(e);
     if (h->copy_stream) {
         cudaStreamSynchronize(h->copy_stream);

@@ -21,6 +21,12 @@
  *    the result is in host memory; device calls are asynchronous on `stream`.
  *  - `stream` is a cudaStream_t: NULL = the handle's own stream; the
  *    special handles cudaStreamLegacy / cudaStreamPerThread are accepted.
+ *    Inside one call the library may fork work onto a second stream of the
+ *    handle (the pair correction of a solve, forked from `stream` after the
+ *    spread and joined back before the call's last kernel; not while
+ *    `stream` is being captured into a CUDA graph), so the call stays
+ *    ordered on `stream` as a whole. FFCM_OVERLAP_PAIRS=0 in the environment
+ *    at ffcm_create keeps every kernel on `stream`.
  *  - Index buffers exchanged through ffcm_get_buffer/ffcm_set_buffer are
  *    1-based, as in the reference (`original_index`, `cell_start`,
  *    `cell_end`); cell hashes are 0-based as in the reference.

@@ -289,6 +289,37 @@ def test_fused_and_unfused_paths_agree(ffcm, monkeypatch):
     assert rel_l2(Vc, Vd) < 1e-6
 
 
+@pytest.mark.parametrize("T", TS)
+def test_side_stream_correction_matches_single_stream(ffcm, monkeypatch, T):
+    """A fused solve outside stream capture runs the pair correction on the
+    configuration's second stream beside the y/z passes and the
+    interpolation and joins it before the last kernel; with
+    FFCM_OVERLAP_PAIRS=0 everything stays on the solve's stream. Both give
+    the same velocities (the same arithmetic; only the interpolation's float
+    atomics reorder), for the plain solve, the fixed-position operator, and
+    repeated calls that reuse the side stream, and both match the oracle."""
+    z = np.load(GOLDEN / "uniform_N2000_64.npz")
+    tag = "f32" if T is np.float32 else "f64"
+    Y, F = z[f"{tag}_Y"], z[f"{tag}_F"]
+    kw = kw_of(40.0, 2000, 64, R_c=3.0)
+    side = ffcm.FFCMConfig(T, **kw)
+    monkeypatch.setenv("FFCM_OVERLAP_PAIRS", "0")
+    single = ffcm.FFCMConfig(T, **kw)
+    monkeypatch.delenv("FFCM_OVERLAP_PAIRS")
+    Vs = _run(ffcm, single, Y, F)
+    bound = 1e-6 if T is np.float32 else 1e-13
+    for _ in range(3):
+        assert rel_l2(_run(ffcm, side, Y, F), Vs) < bound
+    ora = O.OracleConfig(T, **kw)
+    assert rel_l2(Vs, O.apply(ora, Y, F)) < (1e-5 if T is np.float32 else 1e-10)
+    rng = np.random.default_rng(41)
+    op_side = ffcm.FFCMMobility(side, Y)
+    op_single = ffcm.FFCMMobility(single, Y)
+    for _ in range(2):
+        G = rng.standard_normal((2000, 3)).astype(T)
+        assert rel_l2(op_side @ G, op_single @ G) < bound
+
+
 def test_configurations_of_different_sizes_alive_at_once(ffcm):
     """Kernel launch limits are per process, not per configuration: a smaller
     configuration created later must not break an earlier, larger one."""
