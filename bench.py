@@ -322,7 +322,8 @@ def run_reference(args, rank, world):
 
 
 def secondary_workloads(args, local_rank):
-    """Batched, adjoint and clustered measurements for the single-GPU line."""
+    """Batched, adjoint, clustered and resistance measurements for the
+    single-GPU line."""
     import copy
     out = {}
     keep = {
@@ -335,8 +336,12 @@ def secondary_workloads(args, local_rank):
         "clustered": ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config",
                       "fixed_position_operator_ms_per_rhs", "gradient_ms_per_rhs", "stage_ms", "tuning", "e2e",
                       "roofline", "clocks", "gpu_launches"),
+        "resistance": ("metric", "value", "unit", "ms_per_step", "steps", "warmup", "config", "iterations",
+                       "solves_per_s", "ms_per_iteration", "apply_ms", "cg_overhead_per_iteration_ms", "e2e",
+                       "roofline", "iteration_roofline", "clocks", "gpu_launches"),
     }
-    runs = (("batched", measure_batched, 10), ("adjoint", measure_adjoint, 10), ("clustered", measure_clustered, 3))
+    runs = (("batched", measure_batched, 10), ("adjoint", measure_adjoint, 10), ("clustered", measure_clustered, 3),
+            ("resistance", lambda *a: measure_resistance(*a)[0], 2))
     for name, fn, steps in runs:
         a = copy.copy(args)
         a.steps, a.warmup, a.skip_cpu_baseline = steps, 3, True
@@ -1018,6 +1023,18 @@ def resistance_inputs():
 
 
 def run_resistance(args, rank, world, local_rank):
+    line, dist = measure_resistance(args, rank, world, local_rank)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def measure_resistance(args, rank, world, local_rank):
+    """The resistance solve's line (rank 0; None elsewhere) and the process
+    group (None on one GPU)."""
     import torch
     ffcm = _load_product()
     torch.cuda.set_device(local_rank)
@@ -1138,17 +1155,10 @@ def run_resistance(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "gpu_launches": int(launches),
         }
+    else:
+        line = None
     cfg.close()
-    if rank == 0 and world == 1 and not args.no_extras:
-        # the secondary workloads on the same box, each with its own CUDA-event
-        # time, clocks and roofline, at reduced step counts
-        line.update(secondary_workloads(args, local_rank))
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
-    return 0
+    return line, dist
 
 
 SPLIT_METRIC = "particles/s per mobility solve of one system split over the GPUs by z slabs (N=500k, 512^3, Float32)"
@@ -1293,7 +1303,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--skip-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true",
-                    help="plain workload only: no batched/adjoint/clustered sub-objects")
+                    help="plain workload only: no batched/adjoint/clustered/resistance sub-objects")
     ap.add_argument("--workload", choices=["plain", "batched", "adjoint", "clustered", "resistance", "split"], default="plain")
     ap.add_argument("--grid", default=None,
                     help="Mx,My,Mz: smaller case at the same spacing and density (profiling)")

@@ -312,13 +312,18 @@ struct ffcm_handle {
     // positions are sorted (created on first use)
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_ready = nullptr, ev_forces = nullptr;
-    // fused solves outside stream capture: the pair correction runs on
+    // fused solves outside stream capture: the pair correction may run on
     // side_stream beside the grid stages (fork after the spread, join before
-    // the last kernel; created on first use). FFCM_OVERLAP_PAIRS=0 keeps it
-    // on the solve's stream.
-    bool overlap_pairs = true;
+    // the last kernel; created on first use). overlap_pairs: 1 always, 0
+    // never (FFCM_OVERLAP_PAIRS=1 / 0), -1 decided by the first solve's
+    // timings (pair_probe: 0 not started, 1 probe events recorded, 2
+    // decided; pair_overlap the decision).
+    int overlap_pairs = -1;
+    int pair_probe = 0;
+    bool pair_overlap = false;
     cudaStream_t side_stream = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_probe[4] = {nullptr, nullptr, nullptr, nullptr};   // y forward, correction
     int* d_err = nullptr;
     int* h_err = nullptr;
     int64_t launches = 0;
@@ -1118,7 +1123,9 @@ struct Engine final : EngineBase {
     // three passes run chunk by chunk, so a chunk's intermediate spectrum
     // (3 My Mz kx_chunk values) stays in L2 between the passes and only the
     // first read and the last write of each value reach HBM.
-    int stokes_yz(cudaStream_t s) {
+    // probe: events recorded on s before and after the y forward pass
+    // (probe[0], probe[1]; the unchunked sequence only).
+    int stokes_yz(cudaStream_t s, cudaEvent_t* probe = nullptr) {
         if (kx_chunk > 0 && kx_chunk < nkx) {
             StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
             for (int k0 = 0; k0 < nkx; k0 += kx_chunk) {
@@ -1131,7 +1138,9 @@ struct Engine final : EngineBase {
         }
         {
             StageScope sc(h, FFCM_STAGE_FFT_Y_FWD, s);
+            if (probe) CUDA_TRY(cudaEventRecord(probe[0], s));
             TRY(launch_y(s, 0));
+            if (probe) CUDA_TRY(cudaEventRecord(probe[1], s));
         }
         {
             StageScope sc(h, FFCM_STAGE_FFT_Z_STOKES, s);
@@ -1203,39 +1212,81 @@ struct Engine final : EngineBase {
             return correct(V, s);
         }
         TRY(spread_to_spectrum(s, nullptr, build_lists));
-        bool side = false;
-        TRY(fork_pairs(s, side));
-        TRY(stokes_yz(s));
+        bool side = false, probe = false;
+        TRY(fork_pairs(s, side, probe));
+        TRY(stokes_yz(s, probe ? h->ev_probe : nullptr));
         if (keep_u) {
             StageScope sc(h, FFCM_STAGE_FFT_X_INV, s);
             TRY(x_inverse(gu, s));
         }
         TRY(interp_from_spectrum(s));
         if (side) {
-            // (the correction stage's time is the pair kernel's, on the side stream)
+            // (the correction stage's time is the side stream's pair kernel's)
             CUDA_TRY(cudaStreamWaitEvent(s, h->ev_join, 0));
             return launch(h, k_finish_velocity<T>, grid_for(N, 256), 256, 0, s, N, (const int32_t*)perm,
                           (const T*)partial, (const T*)dvs, h3, static_cast<T*>(V));
         }
         StageScope sc(h, FFCM_STAGE_CORRECT, s);
-        return launch(h, corr_tpp(N) == 4 ? k_correct<T, 4> : k_correct<T, 1>, grid_for((int64_t)N * corr_tpp(N), 128), 128, 0, s, N, (const vec4<T>*)Ys,
-                      (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
-                      static_cast<T*>(V), cc, (const T*)partial, h3);
+        if (probe) CUDA_TRY(cudaEventRecord(h->ev_probe[2], s));
+        TRY(launch(h, corr_tpp(N) == 4 ? k_correct<T, 4> : k_correct<T, 1>, grid_for((int64_t)N * corr_tpp(N), 128), 128, 0, s, N, (const vec4<T>*)Ys,
+                   (const vec4<T>*)Fs, (const int32_t*)off, (const int32_t*)perm,
+                   static_cast<T*>(V), cc, (const T*)partial, h3));
+        if (probe) CUDA_TRY(cudaEventRecord(h->ev_probe[3], s));
+        return FFCM_OK;
     }
 
     // The pair correction depends only on the sorted particles and the cell
-    // list, so outside stream capture it runs on the handle's side stream
+    // list, so outside stream capture it can run on the handle's side stream
     // while the y/z passes and the interpolation run on s: the fork follows
     // the spread (the y pass leaves a third of each SM's registers free, the
-    // spread none), the join precedes k_finish_velocity. `side` tells the
-    // caller whether it forked. Under capture (the batched graph, the CG
-    // loop) the solve keeps the single-stream order.
-    int fork_pairs(cudaStream_t s, bool& side) {
+    // spread none), the join precedes k_finish_velocity. That pays while the
+    // correction is short next to a y pass (it then runs in the y pass's
+    // spare registers: 0.16 against 0.62 ms at 512^3, 10% by volume), and
+    // costs when it is long (dense clusters: 7.7 against 6.0 ms at 1024^3,
+    // where it slows the z pass by about its own time). So unless
+    // FFCM_OVERLAP_PAIRS forces a mode, the first solve runs on one stream
+    // with events around its y forward pass and its correction, and a later
+    // solve, once those have completed, fixes the mode for the configuration:
+    // overlap when the correction took under half the y pass. `side` tells
+    // the caller whether it forked, `probe` whether to record the events
+    // (ev_probe[0..1] around the y forward pass, [2..3] around k_correct).
+    // Under capture (the batched graph, the CG loop) the solve keeps the
+    // single-stream order.
+    int fork_pairs(cudaStream_t s, bool& side, bool& probe) {
         side = false;
-        if (!h->overlap_pairs) return FFCM_OK;
+        probe = false;
+        if (h->overlap_pairs == 0) return FFCM_OK;
         cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
         CUDA_TRY(cudaStreamIsCapturing(s, &cap));
         if (cap != cudaStreamCaptureStatusNone) return FFCM_OK;
+        if (h->overlap_pairs < 0) {
+            if (h->pair_probe == 0) {
+                if (kx_chunk > 0 && kx_chunk < nkx) {   // chunked y/z/y: no lone y pass to time
+                    h->pair_probe = 2;
+                    h->pair_overlap = false;
+                    return FFCM_OK;
+                }
+                for (cudaEvent_t& e : h->ev_probe)
+                    if (!e) CUDA_TRY(cudaEventCreate(&e));
+                h->pair_probe = 1;
+                probe = true;
+                return FFCM_OK;
+            }
+            if (h->pair_probe == 1) {
+                const cudaError_t q = cudaEventQuery(h->ev_probe[3]);
+                if (q == cudaErrorNotReady) {
+                    (void)cudaGetLastError();   // not an error: the probe solve is still running
+                    return FFCM_OK;
+                }
+                CUDA_TRY(q);
+                float ty = 0, tc = 0;
+                CUDA_TRY(cudaEventElapsedTime(&ty, h->ev_probe[0], h->ev_probe[1]));
+                CUDA_TRY(cudaEventElapsedTime(&tc, h->ev_probe[2], h->ev_probe[3]));
+                h->pair_overlap = tc < 0.5f * ty;
+                h->pair_probe = 2;
+            }
+            if (!h->pair_overlap) return FFCM_OK;
+        }
         if (!dvs) TRY(alloc(dvs, 3 * (size_t)N));
         if (!h->side_stream) {
             CUDA_TRY(cudaStreamCreateWithFlags(&h->side_stream, cudaStreamNonBlocking));
@@ -1826,7 +1877,9 @@ static int create_handle(ffcm_handle** out, int32_t dtype, const double* L, doub
     }
     {
         const char* v = std::getenv("FFCM_OVERLAP_PAIRS");
-        if (v && std::strcmp(v, "0") == 0) h->overlap_pairs = false;
+        if (v && std::strcmp(v, "0") == 0) h->overlap_pairs = 0;
+        else if (v && std::strcmp(v, "1") == 0) h->overlap_pairs = 1;
+        else if (v && *v) return fail(FFCM_ERR_ARGUMENT, "FFCM_OVERLAP_PAIRS must be \"0\" or \"1\"");
     }
     CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CUDA_TRY(cudaMalloc(&h->d_err, sizeof(int)));
@@ -1959,6 +2012,8 @@ int ffcm_destroy(ffcm_handle* h) {
     if (h->side_stream) cudaStreamDestroy(h->side_stream);
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
+    for (cudaEvent_t e : h->ev_probe)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : h->events) cudaEventDestroy(e);
     if (h->copy_stream) {
         cudaStreamSynchronize(h->copy_stream);

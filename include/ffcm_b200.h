@@ -25,8 +25,10 @@
  *    handle (the pair correction of a solve, forked from `stream` after the
  *    spread and joined back before the call's last kernel; not while
  *    `stream` is being captured into a CUDA graph), so the call stays
- *    ordered on `stream` as a whole. FFCM_OVERLAP_PAIRS=0 in the environment
- *    at ffcm_create keeps every kernel on `stream`.
+ *    ordered on `stream` as a whole. A handle's first solve times its
+ *    correction against its y pass and later solves fork only when the
+ *    correction is the shorter by half; FFCM_OVERLAP_PAIRS=0 (never) or 1
+ *    (always) in the environment at ffcm_create overrides that.
  *  - Index buffers exchanged through ffcm_get_buffer/ffcm_set_buffer are
  *    1-based, as in the reference (`original_index`, `cell_start`,
  *    `cell_end`); cell hashes are 0-based as in the reference.

@@ -105,11 +105,14 @@ def test_cg_repeats_and_memory_paths_agree(ffcm, T):
 
     def agree(Fa, ha, Fb, hb):
         # same iteration count: agreement to rounding amplified by the
-        # iteration (F64: ~1e-16 x condition x iterations); one more iteration
-        # on one side: agreement to the stopping tolerance sqrt(eps)
+        # iteration (F64: ~1e-16 x condition x iterations); a few iterations
+        # apart (F32, where the atomics' order moves the count by up to a few:
+        # 44 and 46 have been seen for this system) or one apart (F64):
+        # agreement to the stopping tolerance sqrt(eps)
         if ha.iters == hb.iters:
             return rel_l2(Fa, Fb) < (1e-4 if T == np.float32 else 1e-9)
-        return abs(ha.iters - hb.iters) == 1 and rel_l2(Fa, Fb) < (2e-3 if T == np.float32 else 1e-7)
+        apart = 3 if T == np.float32 else 1
+        return abs(ha.iters - hb.iters) <= apart and rel_l2(Fa, Fb) < (2e-3 if T == np.float32 else 1e-7)
 
     F1, h1 = ffcm.cg(op, V, log=True)
     F2, h2 = ffcm.cg(op, V, log=True)

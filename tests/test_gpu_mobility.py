@@ -290,34 +290,55 @@ def test_fused_and_unfused_paths_agree(ffcm, monkeypatch):
 
 
 @pytest.mark.parametrize("T", TS)
-def test_side_stream_correction_matches_single_stream(ffcm, monkeypatch, T):
-    """A fused solve outside stream capture runs the pair correction on the
-    configuration's second stream beside the y/z passes and the
-    interpolation and joins it before the last kernel; with
+@pytest.mark.parametrize("case", ["uniform", "cluster"])
+def test_side_stream_correction_matches_single_stream(ffcm, monkeypatch, T, case):
+    """A fused solve outside stream capture may run the pair correction on
+    the configuration's second stream beside the y/z passes and the
+    interpolation and join it before the last kernel (FFCM_OVERLAP_PAIRS=1
+    forces that here; left unset, the first solve's timings decide); with
     FFCM_OVERLAP_PAIRS=0 everything stays on the solve's stream. Both give
     the same velocities (the same arithmetic; only the interpolation's float
     atomics reorder), for the plain solve, the fixed-position operator, and
-    repeated calls that reuse the side stream, and both match the oracle."""
-    z = np.load(GOLDEN / "uniform_N2000_64.npz")
-    tag = "f32" if T is np.float32 else "f64"
-    Y, F = z[f"{tag}_Y"], z[f"{tag}_F"]
-    kw = kw_of(40.0, 2000, 64, R_c=3.0)
+    repeated calls that reuse the side stream, and both match the oracle.
+    `cluster` puts 600 of 3000 particles in one tight cluster (cells of
+    dozens)."""
+    if case == "uniform":
+        z = np.load(GOLDEN / "uniform_N2000_64.npz")
+        tag = "f32" if T is np.float32 else "f64"
+        Y, F = z[f"{tag}_Y"], z[f"{tag}_F"]
+        kw = kw_of(40.0, 2000, 64, R_c=3.0)
+    else:
+        rng = np.random.default_rng(3000)
+        Y = rng.random((3000, 3)) * 40.0
+        Y[:600] = 20.0 + rng.standard_normal((600, 3)) * 1.5
+        Y, F = Y.astype(T), rng.standard_normal((3000, 3)).astype(T)
+        kw = kw_of(40.0, 3000, 64, R_c=3.0)
+    N = Y.shape[0]
+    monkeypatch.setenv("FFCM_OVERLAP_PAIRS", "1")
     side = ffcm.FFCMConfig(T, **kw)
     monkeypatch.setenv("FFCM_OVERLAP_PAIRS", "0")
     single = ffcm.FFCMConfig(T, **kw)
     monkeypatch.delenv("FFCM_OVERLAP_PAIRS")
+    adaptive = ffcm.FFCMConfig(T, **kw)
     Vs = _run(ffcm, single, Y, F)
     bound = 1e-6 if T is np.float32 else 1e-13
     for _ in range(3):
         assert rel_l2(_run(ffcm, side, Y, F), Vs) < bound
+        assert rel_l2(_run(ffcm, adaptive, Y, F), Vs) < bound   # probe solve, then its decision
     ora = O.OracleConfig(T, **kw)
     assert rel_l2(Vs, O.apply(ora, Y, F)) < (1e-5 if T is np.float32 else 1e-10)
     rng = np.random.default_rng(41)
     op_side = ffcm.FFCMMobility(side, Y)
     op_single = ffcm.FFCMMobility(single, Y)
     for _ in range(2):
-        G = rng.standard_normal((2000, 3)).astype(T)
+        G = rng.standard_normal((N, 3)).astype(T)
         assert rel_l2(op_side @ G, op_single @ G) < bound
+
+
+def test_overlap_setting_is_validated(ffcm, monkeypatch):
+    monkeypatch.setenv("FFCM_OVERLAP_PAIRS", "yes")
+    with pytest.raises(ffcm.ArgumentError):
+        ffcm.FFCMConfig(np.float32, **kw_of(40.0, 2000, 64, R_c=3.0))
 
 
 def test_configurations_of_different_sizes_alive_at_once(ffcm):
