@@ -305,6 +305,12 @@ def run_reference(args, rank, world):
         units, unit, metric, config = Y.shape[0], UNIT, METRIC, workload_config()
         sample = (f"{warm} warm-up + {steps} timed full solves of the workload by the C/pocketfft "
                   f"restatement of the reference CPU path (Julia is not installed)")
+    if "parallelism" not in config:
+        # the same key as the GPU arm's line for this workload and world size
+        par = "replicas" if world > 1 else "single"
+        if args.workload == "batched" and world > 1:
+            par = "systems sharded across ranks"
+        config = {**config, "parallelism": par}
     for _ in range(warm):
         fn()
     ts = [fn() for _ in range(steps)]
